@@ -1,0 +1,550 @@
+// Per-pixel hash-table build: projection, counting sort by pixel, bucket order.
+//
+// Replaces NeuralPoints.pts2plane (epcq/epcq.py:279-295) + _C.scatter_hashtable
+// (epcq/csrc/rasterization.cu:130-171).  The reference projects with two cuBLAS
+// GEMMs, radix-sorts all N pixel ids with torch.sort, and then has one thread
+// per pixel binary-search the sorted array and copy its run.  Here the pixel
+// ids are a small dense key range, so the sort is a counting sort:
+//
+//   k_project_count   one pass over xyz: pixel id + depth with the reference's
+//                     exact rounding, atomic slot within the pixel's bucket
+//   k_block_sums      per-block totals of the H*W counts
+//   k_scan_hash       exclusive scan -> hash_table (start, count) / (-1, -1)
+//   k_scatter         every point to start + slot; -1 into the off-image tail
+//   k_sort_small      buckets of 2..16 entries sorted in registers by a
+//                     bitonic network (thread per pixel)
+//   k_sort_deep       larger buckets: one CTA at a time, bitonic sort in
+//                     shared memory (<= 2048 entries) or in place in global memory
+//
+// The atomic slots make the order inside a bucket arbitrary; the per-bucket
+// sort restores the reference's order: ascending point id (the stable sort's
+// order) when sort == 0, (depth, id) when sort != 0 (its stable bubble sort).
+#include <cstdio>
+
+#include "hp_common.cuh"
+
+namespace hp {
+
+constexpr int kSmallBucket = 16;
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;                    // counts per thread in the scan
+constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr int kDeepSmem = 2048;                  // entries a CTA sorts in shared memory
+constexpr int kDeepThreads = 256;
+
+// Bucket sort key: the point id (sort == 0) or (depth, id) with depth mapped to
+// an order-preserving integer (-0.0 folded onto +0.0 as float comparison does).
+__device__ __forceinline__ unsigned long long sort_key(int id, float depth, int by_depth) {
+  if (!by_depth) return (unsigned long long)(unsigned)id;
+  unsigned b = __float_as_uint(depth == 0.0f ? 0.0f : depth);
+  b = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+  return ((unsigned long long)b << 32) | (unsigned)id;
+}
+
+// ---------------------------------------------------------------------------
+// projection + count (epcq.py:251-274 restated with the GEMMs' rounding)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_project_count(const float* __restrict__ xyz, int n,
+                                                       const float* __restrict__ w2c, const float* __restrict__ K,
+                                                       int H, int W, int fused_world, int fused_image,
+                                                       int* __restrict__ counts, int2* __restrict__ pid_slot,
+                                                       float* __restrict__ depth_out) {
+  float w[12], k[9];
+#pragma unroll
+  for (int i = 0; i < 12; i++) w[i] = __ldg(w2c + i);
+#pragma unroll
+  for (int i = 0; i < 9; i++) k[i] = __ldg(K + i);
+  const int hw = H * W;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float x = __ldg(xyz + 3 * (size_t)i), y = __ldg(xyz + 3 * (size_t)i + 1),
+                z = __ldg(xyz + 3 * (size_t)i + 2);
+    float pc[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      const float* a = w + 4 * r;
+      const float g = fused_world ? __fmaf_rn(a[2], z, __fmaf_rn(a[1], y, __fmul_rn(a[0], x)))
+                                  : __fadd_rn(__fadd_rn(__fmul_rn(a[0], x), __fmul_rn(a[1], y)), __fmul_rn(a[2], z));
+      pc[r] = __fadd_rn(g, a[3]);
+    }
+    float s[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      const float* a = k + 3 * r;
+      s[r] = fused_image ? __fmaf_rn(a[2], pc[2], __fmaf_rn(a[1], pc[1], __fmul_rn(a[0], pc[0])))
+                         : __fadd_rn(__fadd_rn(__fmul_rn(a[0], pc[0]), __fmul_rn(a[1], pc[1])), __fmul_rn(a[2], pc[2]));
+    }
+    const int ix = __float2int_rz(__fdiv_rn(s[0], s[2]));
+    const int iy = __float2int_rz(__fdiv_rn(s[1], s[2]));
+    const bool inb = 0 <= ix && ix < W && 0 <= iy && iy < H;
+    const int p = inb ? ix + iy * W : hw;
+    const int slot = inb ? atomicAdd(counts + p, 1) : 0;
+    pid_slot[i] = make_int2(p, slot);
+    depth_out[i] = pc[2];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// scan over the per-pixel counts
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int block_reduce_sum(int v, int* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  v = lane < nw ? sh[lane] : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_block_sums(const int* __restrict__ counts, int hw,
+                                                             int* __restrict__ block_sums) {
+  __shared__ int sh[32];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; j++)
+    if (base + j < hw) s += counts[base + j];
+  s = block_reduce_sum(s, sh);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = s;
+}
+
+// Exclusive scan of counts -> hash_table; the block's carry-in is the sum of
+// the preceding blocks' totals.
+__global__ void __launch_bounds__(kScanThreads) k_scan_hash(const int* __restrict__ counts, int hw,
+                                                            const int* __restrict__ block_sums,
+                                                            int2* __restrict__ hash, int* __restrict__ scalars) {
+  __shared__ int sh[32];
+  __shared__ int warp_tot[32];
+  int carry = 0;
+  for (int b = threadIdx.x; b < blockIdx.x; b += blockDim.x) carry += block_sums[b];
+  carry = block_reduce_sum(carry, sh);
+
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int c[kScanItems];
+  int local = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; j++) {
+    c[j] = base + j < hw ? counts[base + j] : 0;
+    local += c[j];
+  }
+  // block exclusive scan of `local`
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int wt = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+    int wi = wt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    warp_tot[lane] = wi - wt;
+  }
+  __syncthreads();
+  int off = carry + warp_tot[warp] + incl - local;
+#pragma unroll
+  for (int j = 0; j < kScanItems; j++) {
+    const int p = base + j;
+    if (p < hw) {
+      hash[p] = c[j] > 0 ? make_int2(off, c[j]) : make_int2(-1, -1);
+    }
+    off += c[j];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) scalars[0] = off;  // points inside the image
+}
+
+// ---------------------------------------------------------------------------
+// scatter into buckets
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_scatter(int n, int hw, const int2* __restrict__ pid_slot,
+                                                 const float* __restrict__ depth, const int2* __restrict__ hash,
+                                                 const int* __restrict__ scalars, int* __restrict__ out_idx,
+                                                 float* __restrict__ out_depth) {
+  const int n_in = scalars[0];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int2 ps = pid_slot[i];
+    if (ps.x < hw) {
+      const int pos = hash[ps.x].x + ps.y;
+      out_idx[pos] = i;
+      out_depth[pos] = depth[i];
+    }
+    if (i >= n_in) {
+      out_idx[i] = -1;
+      out_depth[i] = -1.0f;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// per-bucket order
+// ---------------------------------------------------------------------------
+// Keys are (hi, lo): hi = order-preserving depth bits (or 0 when ordering by
+// id alone), lo = point id, or -- when `gather` is set -- the entry's index in
+// the caller's input, so depth ties keep the input order and the id is read
+// back from gather[lo].  Depth travels with the key.
+struct BucketOrder {
+  int by_depth;
+  const int* gather;  // hp_scatter_hashtable's point_idx input, or nullptr
+};
+
+__device__ __forceinline__ unsigned long long entry_key(const BucketOrder& bo, int id_or_pos, float depth) {
+  return sort_key(id_or_pos, depth, bo.by_depth);
+}
+
+template <int N>
+__device__ __forceinline__ void network_sort(unsigned long long (&key)[N], float (&dep)[N]) {
+  // bitonic sorting network, ascending; all indices compile-time -> registers
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+        const int l = i ^ j;
+        if (l > i) {
+          const bool up = (i & k) == 0;
+          const bool swap = up ? (key[i] > key[l]) : (key[i] < key[l]);
+          if (swap) {
+            const unsigned long long tk = key[i];
+            key[i] = key[l];
+            key[l] = tk;
+            const float td = dep[i];
+            dep[i] = dep[l];
+            dep[l] = td;
+          }
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int key_id(const BucketOrder& bo, unsigned long long key) {
+  const int lo = (int)(unsigned)(key & 0xffffffffull);
+  return bo.gather ? bo.gather[lo] : lo;
+}
+
+// Sort the c (<= N) entries at idx/dep; `first` is their absolute position.
+template <int N>
+__device__ __forceinline__ void sort_bucket_regs(const BucketOrder& bo, int* __restrict__ idx,
+                                                 float* __restrict__ dep_arr, int c, int first) {
+  unsigned long long key[N];
+  float dep[N];
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    if (i < c) {
+      dep[i] = dep_arr[i];
+      key[i] = entry_key(bo, bo.gather ? first + i : idx[i], dep[i]);
+    } else {
+      dep[i] = 0.0f;
+      key[i] = ~0ull;
+    }
+  }
+  network_sort<N>(key, dep);
+#pragma unroll
+  for (int i = 0; i < N; i++)
+    if (i < c) {
+      idx[i] = key_id(bo, key[i]);
+      dep_arr[i] = dep[i];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sort_small(int hw, const int2* __restrict__ hash, int* __restrict__ out_idx,
+                                                    float* __restrict__ out_depth, BucketOrder bo) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= hw) return;
+  const int2 h = hash[p];
+  const int c = h.y;
+  if (c < 2 || c > kSmallBucket) return;
+  int* idx = out_idx + h.x;
+  float* dep = out_depth + h.x;
+  if (c <= 2) {
+    sort_bucket_regs<2>(bo, idx, dep, c, h.x);
+  } else if (c <= 4) {
+    sort_bucket_regs<4>(bo, idx, dep, c, h.x);
+  } else if (c <= 8) {
+    sort_bucket_regs<8>(bo, idx, dep, c, h.x);
+  } else {
+    sort_bucket_regs<16>(bo, idx, dep, c, h.x);
+  }
+}
+
+// Large buckets: each CTA scans a contiguous range of pixels kDeepThreads at a
+// time, queues the deep ones in shared memory and sorts them one by one.
+// Up to kDeepSmem entries are sorted in shared memory (keys + depth); larger
+// buckets are sorted in place in global memory by a bitonic network in its
+// "flip" form (every comparator is ascending towards the larger index, so
+// positions past the bucket act as +inf and are never touched), with keys
+// for the gather mode kept in a per-bucket scratch of the sort itself: the
+// output idx array holds the input positions until the final gather.
+__device__ __forceinline__ void cx_global(const BucketOrder& bo, int* idx, float* dep, int i, int l, int c) {
+  if (l >= c) return;
+  const unsigned long long ki = entry_key(bo, idx[i], dep[i]), kl = entry_key(bo, idx[l], dep[l]);
+  if (ki > kl) {
+    const int t = idx[i];
+    idx[i] = idx[l];
+    idx[l] = t;
+    const float d = dep[i];
+    dep[i] = dep[l];
+    dep[l] = d;
+  }
+}
+
+__global__ void __launch_bounds__(kDeepThreads) k_sort_deep(int hw, const int2* __restrict__ hash,
+                                                            int* __restrict__ out_idx, float* __restrict__ out_depth,
+                                                            BucketOrder bo) {
+  __shared__ unsigned long long sk[kDeepSmem];
+  __shared__ float sd[kDeepSmem];
+  __shared__ int queue[kDeepThreads];
+  __shared__ int qn;
+  const int per = (hw + gridDim.x - 1) / gridDim.x;
+  const int lo = blockIdx.x * per, hi = min(hw, lo + per);
+  for (int base = lo; base < hi; base += blockDim.x) {
+    if (threadIdx.x == 0) qn = 0;
+    __syncthreads();
+    const int p = base + threadIdx.x;
+    if (p < hi && hash[p].y > kSmallBucket) queue[atomicAdd(&qn, 1)] = p;
+    __syncthreads();
+    const int nq = qn;
+    for (int q = 0; q < nq; q++) {
+      const int2 h = hash[queue[q]];
+      const int c = h.y;
+      int* idx = out_idx + h.x;
+      float* dep = out_depth + h.x;
+      int npow = 1;
+      while (npow < c) npow <<= 1;
+      if (c <= kDeepSmem) {
+        for (int i = threadIdx.x; i < npow; i += blockDim.x) {
+          if (i < c) {
+            sd[i] = dep[i];
+            sk[i] = entry_key(bo, bo.gather ? h.x + i : idx[i], sd[i]);
+          } else {
+            sk[i] = ~0ull;
+            sd[i] = 0.0f;
+          }
+        }
+        __syncthreads();
+        for (int k = 2; k <= npow; k <<= 1) {
+          for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < npow; i += blockDim.x) {
+              const int l = i ^ j;
+              if (l > i) {
+                const bool up = (i & k) == 0;
+                const unsigned long long a = sk[i], b = sk[l];
+                if (up ? a > b : a < b) {
+                  sk[i] = b;
+                  sk[l] = a;
+                  const float t = sd[i];
+                  sd[i] = sd[l];
+                  sd[l] = t;
+                }
+              }
+            }
+            __syncthreads();
+          }
+        }
+        for (int i = threadIdx.x; i < c; i += blockDim.x) {
+          idx[i] = key_id(bo, sk[i]);
+          dep[i] = sd[i];
+        }
+      } else {
+        // positions stand in for ids while sorting in the gather mode
+        if (bo.gather)
+          for (int i = threadIdx.x; i < c; i += blockDim.x) idx[i] = h.x + i;
+        __syncthreads();
+        for (int k = 2; k <= npow; k <<= 1) {
+          for (int i = threadIdx.x; i < npow / 2; i += blockDim.x) {
+            const int blk = i / (k >> 1), off = i % (k >> 1);
+            const int a = blk * k + off, b = blk * k + k - 1 - off;
+            if (a < c) cx_global(bo, idx, dep, a, b, c);
+          }
+          __syncthreads();
+          for (int j = k >> 2; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < npow / 2; i += blockDim.x) {
+              const int blk = i / j, off = i % j;
+              const int a = blk * 2 * j + off;
+              if (a < c) cx_global(bo, idx, dep, a, a + j, c);
+            }
+            __syncthreads();
+          }
+        }
+        if (bo.gather)
+          for (int i = threadIdx.x; i < c; i += blockDim.x) idx[i] = bo.gather[idx[i]];
+      }
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// standalone scatter_hashtable over inputs already sorted by pixel id
+// ---------------------------------------------------------------------------
+__global__ void k_fill_hash(int hw, int2* __restrict__ hash) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < hw; p += gridDim.x * blockDim.x) hash[p] = make_int2(-1, -1);
+}
+
+__global__ void __launch_bounds__(256) k_runs(const int* __restrict__ point_idx, const int* __restrict__ point2img,
+                                              const float* __restrict__ depth, int n, int hw,
+                                              int* __restrict__ out_idx, float* __restrict__ out_depth,
+                                              int2* __restrict__ hash) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int p = point2img[i];
+    const bool valid = 0 <= p && p < hw;
+    out_idx[i] = valid ? point_idx[i] : -1;
+    out_depth[i] = valid ? depth[i] : -1.0f;
+    if (valid && (i == 0 || point2img[i - 1] != p)) {
+      int e = i + 1;
+      while (e < n && point2img[e] == p) e++;
+      hash[p] = make_int2(i, e - i);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct BuildLayout {
+  size_t counts, block_sums, pid_slot, depth, scalars, total;
+};
+
+static BuildLayout build_layout(int64_t n, int64_t hw) {
+  BuildLayout L;
+  const int64_t nblk = (hw + kScanTile - 1) / kScanTile;
+  size_t o = 0;
+  L.counts = o;
+  o += align256(sizeof(int) * (size_t)(hw > 0 ? hw : 1));
+  L.block_sums = o;
+  o += align256(sizeof(int) * (size_t)(nblk > 0 ? nblk : 1));
+  L.pid_slot = o;
+  o += align256(sizeof(int2) * (size_t)(n > 0 ? n : 1));
+  L.depth = o;
+  o += align256(sizeof(float) * (size_t)(n > 0 ? n : 1));
+  L.scalars = o;
+  o += 256;
+  L.total = o;
+  return L;
+}
+
+static int grid_for(int64_t n, int threads) {
+  int64_t g = (n + threads - 1) / threads;
+  const int64_t cap = 148 * 16;
+  if (g > cap) g = cap;
+  return (int)(g > 0 ? g : 1);
+}
+
+// Bucket-order fix-up shared by hp_pts2plane and hp_scatter_hashtable.
+static int32_t launch_bucket_sort(int hw, const int2* hash, int* out_idx, float* out_depth, BucketOrder bo,
+                                  cudaStream_t st) {
+  k_sort_small<<<(hw + 255) / 256, 256, 0, st>>>(hw, hash, out_idx, out_depth, bo);
+  if (int32_t rc = check_launch("k_sort_small")) return rc;
+  const int blocks = hw < 148 * 4 * kDeepThreads ? (hw + kDeepThreads - 1) / kDeepThreads : 148 * 4;
+  k_sort_deep<<<blocks, kDeepThreads, 0, st>>>(hw, hash, out_idx, out_depth, bo);
+  return check_launch("k_sort_deep");
+}
+
+}  // namespace hp
+
+using namespace hp;
+
+extern "C" void hp_projection_rounding(int64_t n_points, int32_t* fused_world, int32_t* fused_image) {
+  // Point counts above which torch's cuBLAS GEMM for the 3x3 @ 3xN products of
+  // epcq.py:253 (w2c, transposed xyz operand) and epcq.py:261 (K) used a fused
+  // multiply-add chain on B200; below them it rounded each product separately.
+  if (fused_world) *fused_world = n_points > HP_WORLD_FUSED_ABOVE;
+  if (fused_image) *fused_image = n_points > HP_IMAGE_FUSED_ABOVE;
+}
+
+extern "C" size_t hp_pts2plane_workspace_size(int64_t n_points, int32_t height, int32_t width) {
+  if (n_points < 0 || height <= 0 || width <= 0) return 0;
+  return build_layout(n_points, (int64_t)height * width).total;
+}
+
+extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_camera* cam, int32_t sort,
+                                int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table, void* workspace,
+                                size_t workspace_bytes, hp_stream_t stream) {
+  if (!cam) return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane: cam is NULL");
+  const int H = cam->height, W = cam->width;
+  if (H <= 0 || W <= 0 || (int64_t)H * W >= (1ll << 31))
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane: bad image size %dx%d", H, W);
+  if (n_points < 0 || n_points > (1ll << 30))
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane: n_points %lld out of range", (long long)n_points);
+  if (!cam->w2c || !cam->K) return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane: w2c and K are required");
+  if ((n_points > 0 && (!xyz || !sorted_point_idx || !sorted_depth)) || !hash_table)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane: null input/output pointer");
+  if (((uintptr_t)hash_table & 7) != 0)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane: hash_table must be 8-byte aligned");
+  const int64_t hw = (int64_t)H * W;
+  const BuildLayout L = build_layout(n_points, hw);
+  if (!workspace || workspace_bytes < L.total || ((uintptr_t)workspace & 255) != 0)
+    return set_error(HP_ERR_WORKSPACE, "hp_pts2plane: workspace needs %zu bytes, 256-byte aligned (got %zu)",
+                     L.total, workspace_bytes);
+  cudaStream_t st = (cudaStream_t)stream;
+  char* ws = (char*)workspace;
+  int* counts = (int*)(ws + L.counts);
+  int* block_sums = (int*)(ws + L.block_sums);
+  int2* pid_slot = (int2*)(ws + L.pid_slot);
+  float* depth = (float*)(ws + L.depth);
+  int* scalars = (int*)(ws + L.scalars);
+  int2* hash = (int2*)hash_table;
+  const int n = (int)n_points;
+  int32_t fw, fi;
+  hp_projection_rounding(n_points, &fw, &fi);
+
+  if (cudaMemsetAsync(counts, 0, sizeof(int) * hw, st) != cudaSuccess ||
+      cudaMemsetAsync(scalars, 0, 256, st) != cudaSuccess)
+    return set_error(HP_ERR_CUDA, "hp_pts2plane: cudaMemsetAsync failed: %s", cudaGetErrorString(cudaGetLastError()));
+  if (n > 0) {
+    k_project_count<<<grid_for(n, 256), 256, 0, st>>>(xyz, n, cam->w2c, cam->K, H, W, fw, fi, counts, pid_slot,
+                                                      depth);
+    if (int32_t rc = check_launch("k_project_count")) return rc;
+  }
+  const int nblk = (int)((hw + kScanTile - 1) / kScanTile);
+  k_block_sums<<<nblk, kScanThreads, 0, st>>>(counts, (int)hw, block_sums);
+  if (int32_t rc = check_launch("k_block_sums")) return rc;
+  k_scan_hash<<<nblk, kScanThreads, 0, st>>>(counts, (int)hw, block_sums, hash, scalars);
+  if (int32_t rc = check_launch("k_scan_hash")) return rc;
+  if (n > 0) {
+    k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, (int)hw, pid_slot, depth, hash, scalars, sorted_point_idx,
+                                                sorted_depth);
+    if (int32_t rc = check_launch("k_scatter")) return rc;
+  }
+  return launch_bucket_sort((int)hw, hash, sorted_point_idx, sorted_depth, BucketOrder{sort != 0, nullptr}, st);
+}
+
+extern "C" int32_t hp_scatter_hashtable(const int32_t* point_idx, const int32_t* point2img, const float* depth,
+                                        int64_t n, int32_t height, int32_t width, int32_t sort,
+                                        int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table,
+                                        hp_stream_t stream) {
+  if (height <= 0 || width <= 0 || (int64_t)height * width >= (1ll << 31))
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_scatter_hashtable: bad image size %dx%d", height, width);
+  if (n < 0 || n > (1ll << 30))
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_scatter_hashtable: n %lld out of range", (long long)n);
+  if ((n > 0 && (!point_idx || !point2img || !depth || !sorted_point_idx || !sorted_depth)) || !hash_table)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_scatter_hashtable: null pointer");
+  if (((uintptr_t)hash_table & 7) != 0)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_scatter_hashtable: hash_table must be 8-byte aligned");
+  const int hw = height * width;
+  cudaStream_t st = (cudaStream_t)stream;
+  int2* hash = (int2*)hash_table;
+  k_fill_hash<<<grid_for(hw, 256), 256, 0, st>>>(hw, hash);
+  if (int32_t rc = check_launch("k_fill_hash")) return rc;
+  if (n > 0) {
+    k_runs<<<grid_for(n, 256), 256, 0, st>>>(point_idx, point2img, depth, (int)n, hw, sorted_point_idx, sorted_depth,
+                                             hash);
+    if (int32_t rc = check_launch("k_runs")) return rc;
+  }
+  if (!sort) return HP_OK;
+  return launch_bucket_sort(hw, hash, sorted_point_idx, sorted_depth, BucketOrder{1, point_idx}, st);
+}

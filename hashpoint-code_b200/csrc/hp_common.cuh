@@ -1,0 +1,116 @@
+// Shared device helpers of the B200 HashPoint kernels.
+//
+// Arithmetic that decides which points a ray keeps is written with explicit
+// round-to-nearest intrinsics (__fmaf_rn, __fmul_rn, ...) so nvcc cannot fuse
+// or reorder it: every expression reproduces, bit for bit, the way the
+// reference's kernels round (operand order and fused multiply-adds were
+// established by diffing GPU outputs of the reference's expressions), and the
+// CPU oracle restates the same sequence with fmaf.  CUDA's norm3df, rnorm3df
+// and __expf are called exactly where the reference calls them.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/hashpoint_b200.h"
+
+// Point counts above which torch's cuBLAS GEMMs of the reference projection
+// (epcq/epcq.py:253 world->camera, :261 camera->image) used a fused
+// multiply-add chain on B200; at or below them each product was rounded
+// separately.  Established by diffing torch outputs against both forms.
+#ifndef HP_WORLD_FUSED_ABOVE
+#define HP_WORLD_FUSED_ABOVE 1000
+#endif
+#ifndef HP_IMAGE_FUSED_ABOVE
+#define HP_IMAGE_FUSED_ABOVE 100000
+#endif
+
+namespace hp {
+
+constexpr int kWarp = 32;
+constexpr int kLaneCells = 32;     // window cells one sampling warp of the reference covers (k*k <= 32)
+constexpr int kKeptPerCell = 48;   // kept points per window cell (POINT_BUFFER_SIZE48)
+constexpr int kBins = 128;         // t-histogram bins (MAX_SAMPLE_POINTS_NUM)
+constexpr int kBallBuf = 8;        // ids gathered per sample (POINT_BUFFER_SIZE8)
+constexpr int kQueryPerCell = 32;  // ids gathered per window cell by the ray query (POINT_BUFFER_SIZE)
+constexpr int kMaxKernel = 5;      // largest window side of the sampling path (k*k <= 32)
+
+// Camera as the kernels see it: c2w stays a device pointer (rows 0..2 read).
+struct DevCamera {
+  const float* c2w;
+  float fx, fy, cx, cy;
+  int width, height;
+};
+
+// Options as the kernels see them.
+struct DevOptions {
+  int k;
+  float t_intvl;
+  float radius;
+  int S, P;
+  int num_point_per_ray;
+  float alpha_g, gamma;
+};
+
+struct Ray {
+  float o[3];
+  float d[3];
+  float dd;  // dot(d, d), constant per ray
+};
+
+// dot3 as the reference's _dot3d (cuda_util.cuh:57) rounds under nvcc: fma(a2,b2, fma(a0,b0, a1*b1)).
+__device__ __forceinline__ float dot3(float a0, float a1, float a2, float b0, float b1, float b2) {
+  return __fmaf_rn(a2, b2, __fmaf_rn(a0, b0, __fmul_rn(a1, b1)));
+}
+
+// cam2world_ray (cuda_util.cuh:338-354): x = (u + 0.5 - cx) / fx in double,
+// d_i = fma(c_i0, x, c_i1 * y) + c_i2, normalised with rnorm3df.
+__device__ __forceinline__ void make_ray(const float* __restrict__ c2w, float fx, float fy, float cx, float cy, int u,
+                                         int v, Ray& r) {
+  const float x = (float)(((double)u + 0.5 - (double)cx) / (double)fx);
+  const float y = (float)(((double)v + 0.5 - (double)cy) / (double)fy);
+  float d[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    d[i] = __fadd_rn(__fmaf_rn(c2w[4 * i + 0], x, __fmul_rn(c2w[4 * i + 1], y)), c2w[4 * i + 2]);
+    r.o[i] = c2w[4 * i + 3];
+  }
+  const float rn = rnorm3df(d[0], d[1], d[2]);
+#pragma unroll
+  for (int i = 0; i < 3; i++) r.d[i] = __fmul_rn(d[i], rn);
+  r.dd = dot3(r.d[0], r.d[1], r.d[2], r.d[0], r.d[1], r.d[2]);
+}
+
+// PointRayInterset (cuda_util.cuh:215-236): t = (p-o).d / d.d, proj = fma(t, d, o),
+// dist = norm3df(p - proj).
+__device__ __forceinline__ void intersect(const Ray& r, float px, float py, float pz, float& t, float& dist) {
+  const float s0 = __fsub_rn(px, r.o[0]), s1 = __fsub_rn(py, r.o[1]), s2 = __fsub_rn(pz, r.o[2]);
+  t = __fdiv_rn(dot3(s0, s1, s2, r.d[0], r.d[1], r.d[2]), r.dd);
+  const float e0 = __fsub_rn(px, __fmaf_rn(t, r.d[0], r.o[0]));
+  const float e1 = __fsub_rn(py, __fmaf_rn(t, r.d[1], r.o[1]));
+  const float e2 = __fsub_rn(pz, __fmaf_rn(t, r.d[2], r.o[2]));
+  dist = norm3df(e0, e1, e2);
+}
+
+// calculate_neighbor_uv (cuda_util.cuh:382-388) in exact integer form:
+// offsets ceil((l+1)/k) - ceil(k/2) and l%k - (ceil(k/2)-1), clamped into the image.
+__device__ __forceinline__ void window_cell(int v, int u, int k, int H, int W, int l, int& vv, int& uu) {
+  const int koff = (k + 1) >> 1;
+  const int a = v + (l + k) / k - koff;
+  const int b = u + (l % k) - (koff - 1);
+  vv = min(max(a, 0), H - 1);
+  uu = min(max(b, 0), W - 1);
+}
+
+__device__ __forceinline__ float4 load_point(const float* __restrict__ xyz, int id) {
+  const float* p = xyz + 3 * (size_t)id;
+  return make_float4(__ldg(p), __ldg(p + 1), __ldg(p + 2), 0.f);
+}
+
+}  // namespace hp
+
+// Host-side helpers shared by the entry points (defined in hp_api.cu).
+namespace hp {
+int32_t set_error(int32_t code, const char* fmt, ...);
+int32_t check_launch(const char* what);
+}  // namespace hp

@@ -1,0 +1,259 @@
+"""Drop-in `epcq.epcq` module: the reference's point searching and sampling API.
+
+Mirrors the reference's epcq/epcq.py entry points, tensor layouts and return
+signatures for the search+sample path:
+
+  CameraSpec, RenderOptions (same defaults), NeuralPointsGrads   (:15-145)
+  NeuralPoints(pc_type in {'pointnerf', 'gt_pc', 'pc'})          (:147-221)
+    .pts2plane(cam, opt, pc_xyz=None, sort=False)                (:279-295)
+        -> sorted_point_idx_list int32[N], sorted_depth_list f32[N], hash_table int32[H*W, 2]
+    .render_image_hashtable_topk(cam, opt, idx, depth, hash)      (:297-327)
+        -> sp_xyz f32[H,W,S,3], pc_idx int32[H,W,S,P], sp_t f32[H,W,S], mask bool[H,W,S]
+
+pts2plane runs the projection, the per-pixel counting sort and the bucket
+order in the CUDA library (one call, no torch.sort); render_image_hashtable_topk
+runs the fused search/sample kernel.  Both launch on torch's current stream.
+"""
+import os
+from dataclasses import dataclass
+from typing import Union
+
+import torch
+import torch.nn as nn
+
+from . import utils
+from hashpoint import ops
+
+_C = utils._get_c_extension()
+
+
+def _scalar(v):
+    return v.item() if isinstance(v, torch.Tensor) else v
+
+
+@dataclass
+class CameraSpec:
+    c2w: torch.Tensor
+    w2c: torch.Tensor
+    K: torch.Tensor
+    fx: float
+    fy: float
+    cx: float
+    cy: float
+    width: int
+    height: int
+
+    def _to_cpp(self):
+        spec = _C.CameraSpec()
+        spec.c2w = self.c2w
+        spec.w2c = self.w2c
+        spec.fx, spec.fy, spec.cx, spec.cy = self.fx, self.fy, self.cx, self.cy
+        spec.width, spec.height = self.width, self.height
+        return spec
+
+    @staticmethod
+    def decomposeK(K: torch.Tensor):
+        """(fx, fy, cx, cy) as 0-d tensors, like the reference."""
+        return K[0, 0], K[1, 1], K[0, 2], K[1, 2]
+
+    def _save2torch(self, filename):
+        torch.save({"c2w": self.c2w, "w2c": self.w2c,
+                    **{k: torch.as_tensor(_scalar(getattr(self, k))) for k in
+                       ("fx", "fy", "cx", "cy", "width", "height")}}, filename)
+
+    def pixelidx2hwidx(self, pixelidx):
+        return pixelidx // self.width, pixelidx % self.width
+
+    def hwidx2pixelidx(self, h_idx, w_idx):
+        return h_idx * self.width + w_idx
+
+
+@dataclass
+class RenderOptions:
+    kernel_size: int = 5
+    t_intvl: float = 0.01
+    radius_threshold: float = 0.016
+    sigma_threshold: float = 1e-4
+    background_brightness: float = 1.0
+    stop_threshold: float = 0.001
+    num_sample_points_per_ray: int = 16
+    num_point_cloud_per_sp: int = 4
+    num_point_per_ray: int = 256
+    sdf2weight_gaussian_alpha: float = 0.2
+    sdf2weight_gaussian_gamma: float = 0.9
+    sparsity_loss_w: float = 5e-4
+    topK: int = 8
+
+    _CPP_FIELDS = ("kernel_size", "t_intvl", "radius_threshold", "sigma_threshold", "background_brightness",
+                   "stop_threshold", "num_sample_points_per_ray", "num_point_cloud_per_sp", "num_point_per_ray",
+                   "sdf2weight_gaussian_alpha", "sdf2weight_gaussian_gamma", "topK")
+
+    def _to_cpp(self):
+        opt = _C.RenderOptions()
+        for f in self._CPP_FIELDS:
+            setattr(opt, f, getattr(self, f))
+        return opt
+
+    def _save2torch(self, filename):
+        torch.save({f: torch.as_tensor(getattr(self, f)) for f in self._CPP_FIELDS}, filename)
+
+
+@dataclass
+class NeuralPointsGrads:
+    grad_sigma: torch.Tensor
+    grad_sh: torch.Tensor
+    mask_out: torch.Tensor
+
+    def _to_cpp(self):
+        grads = _C.NeuralPointsGrads()
+        grads.grad_sigma_out = self.grad_sigma
+        grads.grad_sh_out = self.grad_sh
+        grads.mask_out = self.mask_out
+        return grads
+
+
+def _read_ply_xyz_rgb(path):
+    """Vertices (and colours, if present) of a PLY file: float64 [N,3], float64 [N,3] in [0,1] or None.
+
+    Stands in for open3d.io.read_point_cloud, which the reference uses for
+    pc_type='gt_pc' (epcq.py:182) and which is not required here.
+    """
+    import numpy as np
+    with open(path, "rb") as f:
+        header = []
+        while True:
+            line = f.readline().decode("ascii", errors="replace").strip()
+            header.append(line)
+            if line == "end_header":
+                break
+        body = f.read()
+    fmt = [h.split()[1] for h in header if h.startswith("format")][0]
+    n = 0
+    props = []
+    in_vertex = False
+    for h in header:
+        t = h.split()
+        if t[:2] == ["element", "vertex"]:
+            n, in_vertex = int(t[2]), True
+        elif t and t[0] == "element":
+            in_vertex = False
+        elif in_vertex and t and t[0] == "property":
+            props.append((t[2], t[1]))
+    tmap = {"float": "f4", "float32": "f4", "double": "f8", "float64": "f8", "uchar": "u1", "uint8": "u1",
+            "char": "i1", "int8": "i1", "short": "i2", "int16": "i2", "ushort": "u2", "uint16": "u2",
+            "int": "i4", "int32": "i4", "uint": "u4", "uint32": "u4"}
+    if fmt == "ascii":
+        rows = np.array(body.decode("ascii").split(), dtype=np.float64)[: n * len(props)].reshape(n, len(props))
+        cols = {name: rows[:, i] for i, (name, _) in enumerate(props)}
+    else:
+        endian = "<" if fmt == "binary_little_endian" else ">"
+        dt = np.dtype([(name, endian + tmap[typ]) for name, typ in props])
+        arr = np.frombuffer(body, dtype=dt, count=n)
+        cols = {name: arr[name].astype(np.float64) for name, _ in props}
+    xyz = np.stack([cols["x"], cols["y"], cols["z"]], 1)
+    rgb = None
+    if all(c in cols for c in ("red", "green", "blue")):
+        rgb = np.stack([cols["red"], cols["green"], cols["blue"]], 1)
+        if dict(props)["red"] in ("uchar", "uint8"):
+            rgb = rgb / 255.0
+    return xyz, rgb
+
+
+class NeuralPoints(nn.Module):
+    def __init__(self,
+                 basis_dim: int = 9,
+                 device: Union[torch.device, str] = "cuda:0",
+                 pc_type: str = "pointnerf",
+                 gt_pc_path: str = None,
+                 pointnerf_path: str = "pointnerf_ckpt/nerf_synthesis/lego.pth",
+                 alpha: float = 5.0,
+                 points=None):
+        super().__init__()
+        assert pc_type in ["pointnerf", "gt_pc", "pc"]
+        self.pc_type = pc_type
+        if pc_type == "pointnerf":
+            if not str(pointnerf_path).endswith(".pth"):
+                raise ValueError("Unsupported pointnerf_path: {}".format(pointnerf_path))
+            ckpt = torch.load(pointnerf_path)
+            self.xyz_data = nn.Parameter(ckpt["neural_points.xyz"], requires_grad=False)
+            self.rgb_data = nn.Parameter(ckpt["neural_points.points_color"].squeeze(0), requires_grad=True)
+            self.dir_data = nn.Parameter(ckpt["neural_points.points_dir"].squeeze(0), requires_grad=True)
+            self.density_data = nn.Parameter(ckpt["neural_points.points_conf"].squeeze(0), requires_grad=True)
+            self.feat_data = nn.Parameter(ckpt["neural_points.points_embeding"].squeeze(0), requires_grad=True)
+            self.capacity = self.xyz_data.shape[0]
+        elif pc_type == "gt_pc":
+            if gt_pc_path is None:
+                raise ValueError("gt_pc_path is required")
+            xyz, rgb = _read_ply_xyz_rgb(gt_pc_path)
+            self.xyz_data = nn.Parameter(torch.tensor(xyz, dtype=torch.float32, device=device), requires_grad=False)
+            rgb_t = torch.zeros_like(self.xyz_data) if rgb is None else \
+                torch.tensor(rgb, dtype=torch.float32, device=device)
+            self.rgb_data = nn.Parameter(rgb_t, requires_grad=True)
+            self.dir_data = nn.Parameter(torch.zeros_like(self.xyz_data), requires_grad=True)
+            self.capacity = self.xyz_data.shape[0]
+            self.basis_dim = basis_dim
+            self.density_data = nn.Parameter(torch.zeros(self.capacity, 1, dtype=torch.float32, device=device),
+                                             requires_grad=True)
+            self.feat_data = nn.Parameter(torch.zeros(self.capacity, 32, dtype=torch.float32, device=device),
+                                          requires_grad=True)
+        else:
+            assert points is not None
+            self.xyz_data = nn.Parameter(points, requires_grad=False)
+            self.rgb_data = nn.Parameter(torch.zeros_like(points), requires_grad=False)
+            self.dir_data = nn.Parameter(torch.zeros_like(points), requires_grad=False)
+            self.density_data = nn.Parameter(torch.zeros((points.shape[0], 1)), requires_grad=False)
+            self.feat_data = nn.Parameter(torch.zeros_like(points), requires_grad=False)
+            self.capacity = self.xyz_data.shape[0]
+        self.multi_bins_rasterize = _C.scatter
+        self.rasterize_hashtable = _C.scatter_hashtable
+        self.quick_sampling = _C.quick_sampling
+
+    def _to_cpp(self):
+        spec = _C.NeuralPointsSpec()
+        spec.xyz_data = self.xyz_data.data
+        return spec
+
+    def _save2torch(self, filename):
+        torch.save({"density_data": self.density_data.data, "sh_data": self.feat_data.data,
+                    "xyz_data": self.xyz_data.data, "basis_dim": torch.tensor(9)}, filename)
+
+    # -- torch helpers of the reference's projection, kept for callers that use
+    #    them directly (pts2plane below does not: it runs in the CUDA library) --
+    def _world2cam(self, cam: CameraSpec, pc_xyz: torch.Tensor = None):
+        xyz = self.xyz_data if pc_xyz is None else pc_xyz
+        pts_c = (cam.w2c[:3, :3] @ xyz.t() + cam.w2c[:3, 3:4]).t()
+        return pts_c, pts_c[:, 2:3]
+
+    def _cam2image(self, pts_c: torch.Tensor, cam: CameraSpec):
+        scrn = cam.K @ pts_c.t()
+        scrn = scrn / scrn[2:3, :]
+        return scrn[0, :], scrn[1, :], scrn[0, :].to(torch.int32), scrn[1, :].to(torch.int32)
+
+    def _convetpixel(self, screen_x, screen_y, hw):
+        inside = (0 <= screen_x) & (screen_x < hw[1]) & (0 <= screen_y) & (screen_y < hw[0])
+        return torch.where(inside, screen_x + screen_y * hw[1], torch.full_like(screen_x, hw[0] * hw[1]))
+
+    def _uv2ray_index(self, uv, width):
+        return (uv[:, 1] * width + uv[:, 0]).to(torch.int32)
+
+    def pts2plane(self, cam: CameraSpec, opt: RenderOptions, pc_xyz: torch.Tensor = None, sort: bool = False):
+        """Projection + per-pixel hash table (epcq.py:279-295), in one CUDA library call."""
+        xyz = (self.xyz_data if pc_xyz is None else pc_xyz).detach()
+        return ops.pts2plane(xyz, cam.w2c, cam.K, _scalar(cam.height), _scalar(cam.width), sort)
+
+    def render_image_hashtable_topk(self, cam: CameraSpec, opt: RenderOptions,
+                                    sorted_point_idx_list: torch.Tensor,
+                                    sorted_depth_list: torch.Tensor,
+                                    hashtable: torch.Tensor,
+                                    save_variables_for_debug: bool = False):
+        """Window search + sampling + per-sample points (epcq.py:297-327)."""
+        if save_variables_for_debug:
+            out_dir = os.environ.get("EPCQ_DEBUG_DIR", ".")
+            os.makedirs(out_dir, exist_ok=True)
+            torch.save({"sorted_point_idx_list": sorted_point_idx_list}, os.path.join(out_dir, "sorted_point_idx_list.pt"))
+            torch.save({"sorted_depth_list": sorted_depth_list}, os.path.join(out_dir, "sorted_depth_list.pt"))
+            torch.save({"hashtable": hashtable}, os.path.join(out_dir, "hashtable.pt"))
+            self._save2torch(os.path.join(out_dir, "epcq.pt"))
+            cam._save2torch(os.path.join(out_dir, "cam.pt"))
+            opt._save2torch(os.path.join(out_dir, "opt.pt"))
+        return self.quick_sampling(self._to_cpp(), cam._to_cpp(), opt._to_cpp(), sorted_point_idx_list, hashtable)

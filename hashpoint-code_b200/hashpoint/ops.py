@@ -1,0 +1,187 @@
+"""Tensor-level entry points over the C ABI.
+
+Each function validates its tensors the way the reference's TORCH_CHECKs do
+(CUDA, contiguous; epcq/csrc/include/util.hpp:4-9), allocates its outputs with
+torch on the inputs' device, and launches on torch's current CUDA stream.
+Nothing here computes on the CPU: the work is the CUDA library's.
+"""
+import ctypes
+
+import torch
+
+from . import native
+
+_vp = ctypes.c_void_p
+
+
+def _ptr(t):
+    return _vp(t.data_ptr()) if t is not None and t.numel() > 0 else _vp(0)
+
+
+def _stream(device):
+    return _vp(torch.cuda.current_stream(device).cuda_stream)
+
+
+def check_input(t, name, dtype=None):
+    if not isinstance(t, torch.Tensor):
+        raise RuntimeError("%s must be a tensor" % name)
+    if not t.is_cuda:
+        raise RuntimeError("%s must be a CUDA tensor" % name)
+    if not t.is_contiguous():
+        raise RuntimeError("%s must be contiguous" % name)
+    if dtype is not None and t.dtype != dtype:
+        raise RuntimeError("%s must be %s, got %s" % (name, dtype, t.dtype))
+    return t
+
+
+def check_matrix(t, name, rows=3, cols=4):
+    check_input(t, name, torch.float32)
+    if t.dim() != 2 or t.shape[1] != cols or t.shape[0] < rows:
+        raise RuntimeError("%s must be a [>=%d, %d] float32 matrix, got %s" % (name, rows, cols, tuple(t.shape)))
+    return t
+
+
+def make_camera(c2w=None, w2c=None, K=None, fx=0.0, fy=0.0, cx=0.0, cy=0.0, width=0, height=0):
+    """HpCamera over device tensors (the caller keeps the tensors alive)."""
+    cam = native.HpCamera()
+    cam.c2w = _ptr(c2w).value
+    cam.w2c = _ptr(w2c).value
+    cam.K = _ptr(K).value
+    cam.fx, cam.fy, cam.cx, cam.cy = float(fx), float(fy), float(cx), float(cy)
+    cam.width, cam.height = int(width), int(height)
+    return cam
+
+
+def make_options(opt):
+    o = native.HpOptions()
+    o.kernel_size = int(opt.kernel_size)
+    o.t_intvl = float(opt.t_intvl)
+    o.radius_threshold = float(opt.radius_threshold)
+    o.num_sample_points_per_ray = int(opt.num_sample_points_per_ray)
+    o.num_point_cloud_per_sp = int(opt.num_point_cloud_per_sp)
+    o.num_point_per_ray = int(opt.num_point_per_ray)
+    o.sdf2weight_gaussian_alpha = float(opt.sdf2weight_gaussian_alpha)
+    o.sdf2weight_gaussian_gamma = float(opt.sdf2weight_gaussian_gamma)
+    return o
+
+
+def pts2plane(xyz, w2c, K, height, width, sort=False):
+    """Projection + hash table: (sorted_point_idx int32[N], sorted_depth f32[N], hash int32[H*W, 2])."""
+    check_input(xyz, "xyz", torch.float32)
+    if xyz.dim() != 2 or xyz.shape[1] != 3:
+        raise RuntimeError("xyz must be [N, 3], got %s" % (tuple(xyz.shape),))
+    check_matrix(w2c, "w2c")
+    check_input(K, "K", torch.float32)
+    if tuple(K.shape) != (3, 3):
+        raise RuntimeError("K must be [3, 3], got %s" % (tuple(K.shape),))
+    dev = xyz.device
+    H, W = int(height), int(width)
+    n = xyz.shape[0]
+    L = native.lib()
+    ws_bytes = L.hp_pts2plane_workspace_size(n, H, W)
+    if ws_bytes == 0:
+        raise RuntimeError("pts2plane: invalid sizes N=%d H=%d W=%d" % (n, H, W))
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    sidx = torch.empty(n, dtype=torch.int32, device=dev)
+    sdep = torch.empty(n, dtype=torch.float32, device=dev)
+    hsh = torch.empty((H * W, 2), dtype=torch.int32, device=dev)
+    cam = make_camera(w2c=w2c, K=K, width=W, height=H)
+    rc = L.hp_pts2plane(_ptr(xyz), n, ctypes.byref(cam), int(bool(sort)), _ptr(sidx), _ptr(sdep), _ptr(hsh),
+                        _ptr(ws), ws_bytes, _stream(dev))
+    native.check(rc, "hp_pts2plane")
+    return sidx, sdep, hsh
+
+
+def scatter_hashtable(point_idx, point2img, depth, height, width, sort=False):
+    check_input(point_idx, "point_idx_list", torch.int32)
+    check_input(point2img, "point2img_idx_list", torch.int32)
+    check_input(depth, "depth_list", torch.float32)
+    n = point_idx.shape[0]
+    if point2img.shape[0] != n or depth.shape[0] != n:
+        raise RuntimeError("scatter_hashtable: input lengths differ")
+    dev = point_idx.device
+    H, W = int(height), int(width)
+    sidx = torch.empty(n, dtype=torch.int32, device=dev)
+    sdep = torch.empty(n, dtype=torch.float32, device=dev)
+    hsh = torch.empty((H * W, 2), dtype=torch.int32, device=dev)
+    rc = native.lib().hp_scatter_hashtable(_ptr(point_idx), _ptr(point2img), _ptr(depth), n, H, W, int(bool(sort)),
+                                           _ptr(sidx), _ptr(sdep), _ptr(hsh), _stream(dev))
+    native.check(rc, "hp_scatter_hashtable")
+    return sidx, sdep, hsh
+
+
+def _hash_view(hash_table, height, width):
+    check_input(hash_table, "hashtable", torch.int32)
+    if hash_table.dim() == 2:
+        hash_table = hash_table.view(height, width, 2)
+    if hash_table.dim() != 3 or tuple(hash_table.shape) != (height, width, 2):
+        raise RuntimeError("hashtable size error: %s" % (tuple(hash_table.shape),))
+    return hash_table
+
+
+def quick_sampling(xyz, c2w, fx, fy, cx, cy, width, height, opt, sorted_point_idx, hash_table):
+    """(sp_xyz f32[H,W,S,3], pc_idx i32[H,W,S,P], sp_t f32[H,W,S], mask bool[H,W,S])."""
+    check_input(xyz, "xyz_data", torch.float32)
+    check_matrix(c2w, "c2w")
+    check_input(sorted_point_idx, "sorted_point_idx_list", torch.int32)
+    H, W = int(height), int(width)
+    hash_table = _hash_view(hash_table, H, W)
+    dev = xyz.device
+    S, P = int(opt.num_sample_points_per_ray), int(opt.num_point_cloud_per_sp)
+    sp_xyz = torch.empty((H, W, S, 3), dtype=torch.float32, device=dev)
+    pc_idx = torch.empty((H, W, S, P), dtype=torch.int32, device=dev)
+    sp_t = torch.empty((H, W, S), dtype=torch.float32, device=dev)
+    mask = torch.empty((H, W, S), dtype=torch.bool, device=dev)
+    cam = make_camera(c2w=c2w, fx=fx, fy=fy, cx=cx, cy=cy, width=W, height=H)
+    o = make_options(opt)
+    rc = native.lib().hp_quick_sampling(_ptr(xyz), xyz.shape[0], ctypes.byref(cam), ctypes.byref(o),
+                                        _ptr(sorted_point_idx), sorted_point_idx.numel(), _ptr(hash_table),
+                                        _ptr(sp_xyz), _ptr(pc_idx),
+                                        _ptr(sp_t), _ptr(mask), _stream(dev))
+    native.check(rc, "hp_quick_sampling")
+    return sp_xyz, pc_idx, sp_t, mask
+
+
+def quick_query(xyz, c2w, fx, fy, cx, cy, width, height, opt, sorted_point_idx, hash_table, ray_ids):
+    check_input(xyz, "xyz_data", torch.float32)
+    check_matrix(c2w, "c2w")
+    check_input(sorted_point_idx, "sorted_point_idx_list", torch.int32)
+    check_input(ray_ids, "indices_of_ray", torch.int32)
+    H, W = int(height), int(width)
+    hash_table = _hash_view(hash_table, H, W)
+    dev = xyz.device
+    R = ray_ids.shape[0]
+    cap = int(opt.num_point_per_ray)
+    out = torch.full((R, cap), -1, dtype=torch.int32, device=dev) if R == 0 or cap == 0 else \
+        torch.empty((R, cap), dtype=torch.int32, device=dev)
+    cam = make_camera(c2w=c2w, fx=fx, fy=fy, cx=cx, cy=cy, width=W, height=H)
+    o = make_options(opt)
+    rc = native.lib().hp_quick_query_for_nearby_point(_ptr(xyz), xyz.shape[0], ctypes.byref(cam), ctypes.byref(o),
+                                                      _ptr(sorted_point_idx), sorted_point_idx.numel(),
+                                                      _ptr(hash_table), _ptr(ray_ids), R, _ptr(out), _stream(dev))
+    native.check(rc, "hp_quick_query_for_nearby_point")
+    return out
+
+
+def scatter_multibin(point_idx, point2img, depth, height, width, bins):
+    check_input(point_idx, "point_idx_list", torch.int32)
+    check_input(point2img, "point2img_idx_list", torch.int32)
+    check_input(depth, "depth_list", torch.float32)
+    dev = point_idx.device
+    H, W = int(height), int(width)
+    bd = torch.empty((H * W, int(bins)), dtype=torch.float32, device=dev)
+    bi = torch.empty((H * W, int(bins)), dtype=torch.int32, device=dev)
+    rc = native.lib().hp_scatter(_ptr(point_idx), _ptr(point2img), _ptr(depth), point_idx.shape[0], H, W, int(bins),
+                                 _ptr(bd), _ptr(bi), _stream(dev))
+    native.check(rc, "hp_scatter")
+    return bd, bi
+
+
+def ray_directions(c2w, fx, fy, cx, cy, width, height):
+    check_matrix(c2w, "c2w")
+    H, W = int(height), int(width)
+    out = torch.empty((H * W, 3), dtype=torch.float32, device=c2w.device)
+    cam = make_camera(c2w=c2w, fx=fx, fy=fy, cx=cx, cy=cy, width=W, height=H)
+    rc = native.lib().hp_ray_directions(ctypes.byref(cam), _ptr(out), _stream(c2w.device))
+    native.check(rc, "hp_ray_directions")
+    return out

@@ -1,0 +1,151 @@
+/*
+ * hashpoint_b200 -- C ABI of the B200 (sm_100a) HashPoint point searching and
+ * sampling library.
+ *
+ * Every entry point takes plain device pointers and sizes, runs asynchronously
+ * on the caller's stream and allocates nothing: outputs and scratch
+ * ("workspace") are provided by the caller.  Each returns HP_OK (0) or a
+ * negative HP_ERR_* code; hp_last_error() then describes the failure (the
+ * message is per calling thread).  Launch failures are reported; faults that
+ * happen later on the device surface at the caller's next synchronisation.
+ *
+ * Layouts follow the reference's tensors exactly:
+ *   xyz               float32 [n_points, 3]
+ *   sorted_point_idx  int32   [n_points]     point ids grouped by pixel, -1 tail
+ *   sorted_depth      float32 [n_points]     camera depth of those ids, -1 tail
+ *   hash_table        int32   [H*W, 2]       (start, count) per pixel, (-1,-1) empty
+ *   sp_xyz            float32 [H, W, S, 3]   sample positions (0 when unused)
+ *   pc_idx            int32   [H, W, S, P]   point ids near each sample (-1 when unused)
+ *   sp_t              float32 [H, W, S]      sample depths along the ray (0 when unused)
+ *   mask              uint8   [H, W, S]      1 where a sample was emitted (torch.bool layout)
+ * where S = num_sample_points_per_ray and P = num_point_cloud_per_sp.
+ */
+#ifndef HASHPOINT_B200_H
+#define HASHPOINT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HP_API __attribute__((visibility("default")))
+#else
+#define HP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* hp_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+enum {
+  HP_OK = 0,
+  HP_ERR_INVALID_ARGUMENT = -1, /* null pointer, bad size, unsupported option value */
+  HP_ERR_WORKSPACE = -2,        /* workspace missing or smaller than the *_workspace_size query */
+  HP_ERR_CUDA = -3,             /* a CUDA launch or runtime call failed */
+  HP_ERR_UNSUPPORTED = -4       /* valid input outside what this build supports */
+};
+
+/* Camera of the reference's CameraSpec (epcq/csrc/include/data_spec.hpp:15-31,
+ * epcq/epcq.py:16-37).  c2w / w2c: device pointers to row-major matrices with a
+ * row stride of 4 floats (a [3,4] or [4,4] float32 tensor); rows 0..2 are read.
+ * K: device pointer to the row-major 3x3 intrinsics, read only by the
+ * projection (epcq.py:261); may be NULL for the other entry points. */
+typedef struct hp_camera {
+  const float* c2w;
+  const float* w2c;
+  const float* K;
+  float fx, fy, cx, cy;
+  int32_t width, height;
+} hp_camera;
+
+/* The RenderOptions fields the path reads (data_spec.hpp:49-69, epcq.py:82-96). */
+typedef struct hp_options {
+  int32_t kernel_size;              /* search window side k, 1..5 */
+  float t_intvl;                    /* t-histogram bin width, > 0 */
+  float radius_threshold;           /* ray / ball radius */
+  int32_t num_sample_points_per_ray;/* S >= 1 */
+  int32_t num_point_cloud_per_sp;   /* P >= 1 */
+  int32_t num_point_per_ray;        /* ray-query capacity per ray, >= 0 */
+  float sdf2weight_gaussian_alpha;
+  float sdf2weight_gaussian_gamma;
+} hp_options;
+
+/* Library version (major*10000 + minor*100 + patch). */
+HP_API int32_t hp_version(void);
+
+/* Message for the calling thread's last failing call ("" if none). */
+HP_API const char* hp_last_error(void);
+
+/* Which arithmetic the projection uses for its two 3x3 @ 3xN products at this
+ * point count: 1 = fused multiply-add chain, 0 = separately rounded products.
+ * This reproduces what torch's cuBLAS GEMM did for the reference's projection
+ * (epcq/epcq.py:253,261) on B200, so pixel ids and depths match bit for bit. */
+HP_API void hp_projection_rounding(int64_t n_points, int32_t* fused_world, int32_t* fused_image);
+
+/* Scratch bytes hp_pts2plane needs for this problem size. */
+HP_API size_t hp_pts2plane_workspace_size(int64_t n_points, int32_t height, int32_t width);
+
+/* Projection + per-pixel hash table.  Replaces NeuralPoints.pts2plane
+ * (epcq/epcq.py:279-295: _world2cam :251, _cam2image :259, _convetpixel :267,
+ * torch.sort :284, gathers :285-286) followed by _C.scatter_hashtable
+ * (epcq/csrc/rasterization.cu:130-171).  Buckets list point ids in ascending
+ * id order (sort == 0, the stable sort's order) or by (depth, id) (sort != 0,
+ * the reference's stable bubble sort).  Writes every element of the three
+ * outputs.  n_points <= 2^30. */
+HP_API int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_camera* cam, int32_t sort,
+                     int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table,
+                     void* workspace, size_t workspace_bytes, hp_stream_t stream);
+
+/* Per-pixel hash table from inputs already sorted by pixel id.  Replaces
+ * _C.scatter_hashtable (epcq/csrc/rasterization.cu:130-171, kernel :7-34):
+ * point_idx / point2img / depth [n] sorted by point2img ascending; entries with
+ * point2img outside [0, H*W) are left -1.  Writes every element of the outputs.
+ * n <= 2^30. */
+HP_API int32_t hp_scatter_hashtable(const int32_t* point_idx, const int32_t* point2img, const float* depth, int64_t n,
+                             int32_t height, int32_t width, int32_t sort,
+                             int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table,
+                             hp_stream_t stream);
+
+/* Window search, primary-surface selection, K-sample emission and per-sample
+ * point selection for every pixel ray.  Replaces _C.quick_sampling
+ * (epcq/csrc/epcq_render_topk.cu:341-417: quick_sampling_kernel :82-220 then
+ * quick_search_nearby_pc :10-81).  hash_table may come from hp_pts2plane,
+ * hp_scatter_hashtable or the reference.  Writes every element of the four
+ * outputs (no separate fill is needed).  For P < 8 the first P of the up to 8
+ * selected ids are kept (the reference writes 8 ids into a P-wide row there).
+ * n_sorted is the length of sorted_point_idx: bucket ranges are clipped to it
+ * and ids outside [0, n_points) are skipped, so a malformed hash table cannot
+ * make the kernel read out of bounds. */
+HP_API int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const hp_camera* cam, const hp_options* opt,
+                                 const int32_t* sorted_point_idx, int64_t n_sorted, const int32_t* hash_table,
+                                 float* sp_xyz, int32_t* pc_idx, float* sp_t, uint8_t* mask, hp_stream_t stream);
+
+/* Ray query for a list of pixel rays (linear ids v*W+u).  Replaces
+ * _C.quick_query_for_nearby_point (epcq/csrc/epcq_render_topk.cu:287-339,
+ * kernel :222-283).  out [n_rays, num_point_per_ray]: ids with ray distance
+ * below the radius, at most 32 per window cell, in window-cell then bucket
+ * order (the reference's order is that of its atomics), -1 padded.
+ * kernel_size may be 1..31 here.  Ray ids outside the image give a row of -1. */
+HP_API int32_t hp_quick_query_for_nearby_point(const float* xyz, int64_t n_points, const hp_camera* cam,
+                                               const hp_options* opt, const int32_t* sorted_point_idx,
+                                               int64_t n_sorted, const int32_t* hash_table, const int32_t* ray_ids,
+                                               int64_t n_rays, int32_t* out, hp_stream_t stream);
+
+/* Multi-bin z-buffer: per pixel the `bins` nearest-depth points, ascending.
+ * Replaces _C.scatter (epcq/csrc/rasterization.cu:88-128, kernel :36-86).
+ * Inputs sorted by point2img as for hp_scatter_hashtable.  Points with negative
+ * depth are skipped (the reference never advances past one).  Outputs
+ * [H*W, bins], -1 padded.  1 <= bins <= 64. */
+HP_API int32_t hp_scatter(const int32_t* point_idx, const int32_t* point2img, const float* depth, int64_t n,
+                   int32_t height, int32_t width, int32_t bins, float* buffer_depth, int32_t* buffer_point_index,
+                   hp_stream_t stream);
+
+/* Normalised world-space direction of every pixel's ray, [H*W, 3], exactly as
+ * the sampling kernels compute it (cam2world_ray, cuda_util.cuh:338-354). */
+HP_API int32_t hp_ray_directions(const hp_camera* cam, float* dirs, hp_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HASHPOINT_B200_H */

@@ -1,0 +1,133 @@
+"""The C-ABI library loads and exports every symbol include/hashpoint_b200.h declares.
+
+No compute is launched here: argument validation runs on the host and returns
+before any CUDA call, so these checks need no GPU.
+"""
+import ctypes
+import os
+import re
+
+import pytest
+
+from hashpoint import native
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "hashpoint_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"HP_API\s+[\w\s\*]+?\b(hp_\w+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def L():
+    native.build()
+    return native.lib()
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "hp_quick_sampling" in syms and "hp_pts2plane" in syms
+    assert set(syms) == set(native.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol(L):
+    for s in declared_symbols():
+        assert hasattr(L, s), s
+
+
+def test_version(L):
+    assert L.hp_version() >= 100
+
+
+def test_projection_rounding_matches_oracle(L):
+    import oracle
+    oracle.build()
+    for n in [0, 1, 999, 1000, 1001, 4099, 65536, 99999, 100000, 100001, 1_000_000, 3_000_000]:
+        assert native.projection_rounding(n) == oracle.projection_rounding(n), n
+
+
+def test_workspace_size(L):
+    a = L.hp_pts2plane_workspace_size(1000, 10, 10)
+    b = L.hp_pts2plane_workspace_size(2000, 10, 10)
+    c = L.hp_pts2plane_workspace_size(1000, 100, 100)
+    assert 0 < a < b and a < c
+    assert L.hp_pts2plane_workspace_size(10, 0, 10) == 0
+    assert L.hp_pts2plane_workspace_size(-1, 10, 10) == 0
+
+
+def _cam(w=8, h=8, c2w=0x1000):
+    cam = native.HpCamera()
+    cam.c2w = c2w
+    cam.w2c = c2w
+    cam.K = c2w
+    cam.fx = cam.fy = 10.0
+    cam.cx = cam.cy = 4.0
+    cam.width, cam.height = w, h
+    return cam
+
+
+def _opt(k=3, S=8, P=8, t=0.01):
+    o = native.HpOptions()
+    o.kernel_size, o.t_intvl, o.radius_threshold = k, t, 0.01
+    o.num_sample_points_per_ray, o.num_point_cloud_per_sp, o.num_point_per_ray = S, P, 256
+    o.sdf2weight_gaussian_alpha, o.sdf2weight_gaussian_gamma = 0.2, 0.9
+    return o
+
+
+def _err(L):
+    return L.hp_last_error().decode()
+
+
+@pytest.mark.parametrize("k,S,P,t,msg", [(0, 8, 8, 0.01, "kernel_size"), (6, 8, 8, 0.01, "kernel_size"),
+                                         (3, 0, 8, 0.01, "num_sample_points_per_ray"),
+                                         (3, 8, 0, 0.01, "num_point_cloud_per_sp"), (3, 8, 8, 0.0, "t_intvl")])
+def test_quick_sampling_rejects_bad_options(L, k, S, P, t, msg):
+    p = ctypes.c_void_p(0x1000)
+    rc = L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt(k, S, P, t)), p, 10, p, p, p, p, p, None)
+    assert rc == -1 and msg in _err(L)
+
+
+def test_quick_sampling_rejects_null_and_misaligned(L):
+    p = ctypes.c_void_p(0x1000)
+    assert L.hp_quick_sampling(p, 10, None, ctypes.byref(_opt()), p, 10, p, p, p, p, p, None) == -1
+    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, 10, None, p, p, p, p,
+                               None) == -1
+    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, 10, ctypes.c_void_p(0x1004),
+                               p, p, p, p, None) == -1
+    assert "aligned" in _err(L)
+    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam(w=0)), ctypes.byref(_opt()), p, 10, p, p, p, p, p,
+                               None) == -1
+    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, -1, p, p, p, p, p, None) == -1
+
+
+def test_pts2plane_checks_workspace(L):
+    p = ctypes.c_void_p(0x1000)
+    need = L.hp_pts2plane_workspace_size(10, 8, 8)
+    rc = L.hp_pts2plane(p, 10, ctypes.byref(_cam()), 0, p, p, p, ctypes.c_void_p(0x10000), need - 1, None)
+    assert rc == -2 and "workspace" in _err(L)
+    rc = L.hp_pts2plane(p, 10, ctypes.byref(_cam()), 0, p, p, p, None, need, None)
+    assert rc == -2
+    rc = L.hp_pts2plane(p, 10, ctypes.byref(_cam()), 0, p, p, p, ctypes.c_void_p(0x10010), need, None)
+    assert rc == -2  # not 256-byte aligned
+
+
+def test_query_and_scatter_validation(L):
+    p = ctypes.c_void_p(0x1000)
+    o = _opt(k=32)
+    assert L.hp_quick_query_for_nearby_point(p, 10, ctypes.byref(_cam()), ctypes.byref(o), p, 10, p, p, 4, p,
+                                             None) == -1
+    assert L.hp_scatter(p, p, p, 10, 8, 8, 0, p, p, None) == -1
+    assert L.hp_scatter(p, p, p, 10, 8, 8, 65, p, p, None) == -1
+    assert L.hp_scatter_hashtable(p, p, p, 10, 0, 8, 0, p, p, p, None) == -1
+    # nothing to do: no launch, success
+    o = _opt(k=3)
+    assert L.hp_quick_query_for_nearby_point(p, 10, ctypes.byref(_cam()), ctypes.byref(o), p, 10, p, p, 0, p,
+                                             None) == 0
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    monkeypatch.setattr(native, "_lib", None)
+    monkeypatch.setattr(native, "LIB_PATH", str(tmp_path / "nope.so"))
+    with pytest.raises(native.HashPointError):
+        native.lib()

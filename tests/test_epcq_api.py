@@ -1,0 +1,71 @@
+"""Host-side behaviour of the drop-in `epcq` API (no GPU needed)."""
+import pytest
+import torch
+
+import epcq
+from epcq import epcq as E
+
+
+def test_module_surface():
+    C = E._C
+    for f in ("scatter", "scatter_hashtable", "quick_sampling", "quick_query_for_nearby_point"):
+        assert callable(getattr(C, f))
+    for c in ("CameraSpec", "NeuralPointsSpec", "RenderOptions", "NeuralPointsGrads"):
+        assert isinstance(getattr(C, c), type)
+    assert epcq.NeuralPoints is E.NeuralPoints
+
+
+def test_render_options_defaults_match_reference():
+    o = E.RenderOptions()
+    # epcq/epcq.py:83-96
+    assert (o.kernel_size, o.t_intvl, o.radius_threshold, o.sigma_threshold, o.background_brightness,
+            o.stop_threshold, o.num_sample_points_per_ray, o.num_point_cloud_per_sp, o.num_point_per_ray,
+            o.sdf2weight_gaussian_alpha, o.sdf2weight_gaussian_gamma, o.sparsity_loss_w, o.topK) == \
+        (5, 0.01, 0.016, 1e-4, 1.0, 0.001, 16, 4, 256, 0.2, 0.9, 5e-4, 8)
+
+
+def test_spec_fields_accept_zero_dim_tensors():
+    c = E._C.CameraSpec()
+    c.fx = torch.tensor(555.0)
+    c.cx = 200
+    c.width = torch.tensor(400)
+    c.height = 300.0
+    assert (c.fx, c.cx, c.width, c.height) == (555.0, 200.0, 400, 300)
+    with pytest.raises(AttributeError):
+        c.not_a_field = 1
+    with pytest.raises(TypeError):
+        c.c2w = [1, 2]
+
+
+def test_options_to_cpp_roundtrip():
+    o = E.RenderOptions(kernel_size=3, num_point_cloud_per_sp=8)
+    cpp = o._to_cpp()
+    assert cpp.kernel_size == 3 and cpp.num_point_cloud_per_sp == 8
+    assert abs(cpp.t_intvl - 0.01) < 1e-12
+
+
+def test_cpu_tensors_rejected_like_torch_check():
+    pts = torch.zeros(10, 3)
+    npnt = E.NeuralPoints(pc_type="pc", points=pts)
+    cam = E.CameraSpec(c2w=torch.eye(4), w2c=torch.eye(4), K=torch.eye(3), fx=1.0, fy=1.0, cx=0.0, cy=0.0,
+                       width=4, height=4)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        npnt.pts2plane(cam, E.RenderOptions())
+    with pytest.raises(RuntimeError, match="CUDA"):
+        npnt.render_image_hashtable_topk(cam, E.RenderOptions(), torch.zeros(10, dtype=torch.int32),
+                                         torch.zeros(10), torch.zeros(16, 2, dtype=torch.int32))
+
+
+def test_ply_reader(tmp_path):
+    import numpy as np
+    p = tmp_path / "c.ply"
+    xyz = np.array([[0.0, 1.0, 2.0], [3.0, 4.0, 5.0]], np.float32)
+    rgb = np.array([[255, 0, 0], [0, 255, 0]], np.uint8)
+    hdr = ("ply\nformat binary_little_endian 1.0\nelement vertex 2\nproperty float x\nproperty float y\n"
+           "property float z\nproperty uchar red\nproperty uchar green\nproperty uchar blue\nend_header\n")
+    rec = np.zeros(2, dtype=[("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("r", "u1"), ("g", "u1"), ("b", "u1")])
+    rec["x"], rec["y"], rec["z"] = xyz[:, 0], xyz[:, 1], xyz[:, 2]
+    rec["r"], rec["g"], rec["b"] = rgb[:, 0], rgb[:, 1], rgb[:, 2]
+    p.write_bytes(hdr.encode() + rec.tobytes())
+    a, c = E._read_ply_xyz_rgb(str(p))
+    assert np.allclose(a, xyz) and np.allclose(c, rgb / 255.0)
