@@ -1,0 +1,357 @@
+"""Search+sample throughput benchmark (rays/s) on the 1M-point / 800x800 / 100-view workload.
+
+Workload ("shapes"): 1,000,000 FP32 points area-uniform on 32 random boxes and
+ellipsoids in [-1.5,1.5]^3 (each point also carries an fp16[32] feature the path
+never reads), 100 cameras on a radius-4 sphere looking at the origin,
+800x800 pixels, f=1111, radius 0.008, 5x5 window, K=8 samples, 8 points per
+sample, one launch per view.  Seeded synthetic data (seed 0).
+
+One step = all 100 views through the plain per-view launch: hp_pts2plane
+(projection + per-pixel hash table) then hp_quick_sampling (window search,
+primary-surface selection, sample emission, per-sample points), every output
+written to HBM.  With N GPUs (torchrun) every rank renders its own 100 views
+(weak scaling; no collective on the data path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference algorithm's CPU implementation (the
+oracle port, oracle/hp_oracle.cpp) on this machine's host cores on a bounded
+sample of the same workload, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hashpoint-code_b200"))
+
+METRIC = "rays/s search+sample on 1 B200; served p50/p99 ms vs plain per-view launch"
+UNIT = "rays/s"
+WORKLOAD = "shapes-1M-800x800-100views"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hashpoint", choices=["hashpoint", "reference"])
+    ap.add_argument("--views", type=int, default=100)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def config_dict(args, extra=None):
+    d = {"workload": WORKLOAD, "points": 1_000_000, "width": 800, "height": 800, "views_per_step": args.views,
+         "kernel_size": 5, "radius": 0.008, "samples_per_ray": 8, "points_per_sample": 8,
+         "rays_per_step": 800 * 800 * args.views, "parallelism": "views sharded across ranks (replicas)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle port on the host cores
+# ---------------------------------------------------------------------------
+def cpu_baseline(n_views=3, scene=None):
+    """Oracle (C++ restatement) on `n_views` full views of the workload, all host threads.
+
+    rays/s = rays / (hash-table build time + sampling time), both on the CPU.
+    """
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from hashpoint import synth
+    oracle.build()
+    sc = scene or synth.make_shapes(n_views=max(n_views, 1), with_feat=False)
+    cores = os.cpu_count() or 1
+    total_rays, t_total = 0, 0.0
+    for cam in sc.cameras[:n_views]:
+        oc = oracle.camera_from(cam)
+        t0 = time.perf_counter()
+        oi, od, oh = oracle.pts2plane(sc.xyz, oc, False)
+        oracle.quick_sampling(sc.xyz, oc, sc.options, oi, oh, nthreads=cores)
+        t_total += time.perf_counter() - t0
+        total_rays += cam.width * cam.height
+    return {"value": total_rays / t_total, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "%d full view(s) (800x800, 1M points) of the workload: hash-table build single-threaded, "
+                      "search+sample on %d threads; %.2f s wall" % (n_views, cores, t_total)}
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + ",".join(self.FIELDS),
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == len(self.FIELDS):
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for nm, v in zip(names, r[4:]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# main GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from hashpoint import native, synth
+    from hashpoint.engine import CameraTable, ViewPipeline
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    native.build()
+
+    sc = synth.make_shapes(n_views=args.views, seed=0, with_feat=True)
+    xyz = torch.from_numpy(sc.xyz).to(dev)
+    feat = torch.from_numpy(sc.feat).to(dev)  # resident, never read by the path
+    cams = CameraTable(sc.cameras, dev)
+    pipe = ViewPipeline(len(sc.xyz), 800, 800, sc.options, dev)
+    stream = torch.cuda.Stream(dev)
+    structs = [cams.struct(i) for i in range(cams.n)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    # in-image point count per view (for the algorithmic byte count), outside timing
+    n_in = []
+    with torch.cuda.stream(stream):
+        for s in structs:
+            pipe.build(xyz, s, stream)
+            n_in.append(int((pipe.hash[:, 1].clamp(min=0)).sum().item()))
+
+    S, P = sc.options.num_sample_points_per_ray, sc.options.num_point_cloud_per_sp
+    HW = 800 * 800
+    out_bytes = HW * S * (12 + 4 + 1 + 4 * P)
+    samp_bytes = [16 * ni + 8 * HW + out_bytes for ni in n_in]
+
+    def step(ev_samp=None):
+        for i, s in enumerate(structs):
+            pipe.build(xyz, s, stream)
+            if ev_samp is not None:
+                ev_samp[i][0].record(stream)
+            pipe.sample(xyz, s, stream)
+            if ev_samp is not None:
+                ev_samp[i][1].record(stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    t_wall0 = time.perf_counter()
+    step_ms, samp_ms = [], []
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.fill_(1)  # L2 flushed between steps, outside the step events
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in structs]
+            e0.record(stream)
+            step(ev)
+            e1.record(stream)
+            stream.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            samp_ms.extend(a.elapsed_time(b) for a, b in ev)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    t_wall = time.perf_counter() - t_wall0
+    clk = clocks.stop()
+
+    ms_per_step = sum(step_ms) / len(step_ms)
+    if world > 1:
+        t = torch.tensor([ms_per_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_per_step = float(t.item())
+    rays_per_step = HW * len(structs) * world
+    value = rays_per_step / (ms_per_step * 1e-3)
+
+    # roofline of the dominant kernel (k_quick_sampling)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    samp_avg_ms = sum(samp_ms) / len(samp_ms)
+    achieved = (sum(samp_bytes) / len(samp_bytes)) / (samp_avg_ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        traffic = tr.get("k_quick_sampling", {}).get(WORKLOAD)
+    except (OSError, ValueError):
+        pass
+
+    # end to end through the epcq API with host buffers
+    e2e = run_e2e(args, sc, dev, pipe_hw=HW)
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no public dataset)",
+        "config": config_dict(args, {"l2": "flushed between steps (256 MiB write)",
+                                     "path": "plain per-view launch, preallocated buffers"}),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "k_quick_sampling", "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": sum(samp_bytes) / len(samp_bytes),
+                     "avg_launch_ms": samp_avg_ms},
+        "clocks": clk, "e2e": e2e,
+        "gpu_launches": ViewPipeline.KERNELS_PER_VIEW * len(structs) * args.steps,
+        "wall_s_timed_region": t_wall,
+        "stages_ms_per_view": {"build_plus_sample": ms_per_step / len(structs), "sample": samp_avg_ms},
+    }
+    if rank == 0 and world == 1:
+        result["cpu_baseline"] = cpu_baseline()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    del feat
+
+
+def run_e2e(args, sc, dev, pipe_hw):
+    """The same metric through the public epcq API, inputs copied from pinned host memory every step."""
+    import numpy as np
+    import torch
+
+    from epcq import epcq as E
+
+    xyz_h = torch.from_numpy(sc.xyz).pin_memory()
+    c2w_h = torch.from_numpy(np.stack([c.c2w for c in sc.cameras])).pin_memory()
+    w2c_h = torch.from_numpy(np.stack([c.w2c for c in sc.cameras])).pin_memory()
+    K_h = torch.from_numpy(np.stack([c.K for c in sc.cameras])).pin_memory()
+    opt = E.RenderOptions(kernel_size=5, radius_threshold=0.008, num_sample_points_per_ray=8,
+                          num_point_cloud_per_sp=8)
+    counts_h = torch.empty(len(sc.cameras), dtype=torch.int64).pin_memory()
+    h2d = xyz_h.numel() * 4 + (c2w_h.numel() + w2c_h.numel() + K_h.numel()) * 4
+    d2h = counts_h.numel() * 8
+    model = E.NeuralPoints(pc_type="pc", points=torch.empty_like(xyz_h, device=dev))
+    c2w, w2c, K = (torch.empty_like(t, device=dev) for t in (c2w_h, w2c_h, K_h))
+
+    def one():
+        model.xyz_data.data.copy_(xyz_h, non_blocking=True)
+        c2w.copy_(c2w_h, non_blocking=True)
+        w2c.copy_(w2c_h, non_blocking=True)
+        K.copy_(K_h, non_blocking=True)
+        counts = torch.empty(len(sc.cameras), dtype=torch.int64, device=dev)
+        for i, c in enumerate(sc.cameras):
+            cam = E.CameraSpec(c2w=c2w[i], w2c=w2c[i], K=K[i], fx=c.fx, fy=c.fy, cx=c.cx, cy=c.cy,
+                               width=c.width, height=c.height)
+            idx, dep, hsh = model.pts2plane(cam, opt)
+            sp_xyz, pc_idx, sp_t, mask = model.render_image_hashtable_topk(cam, opt, idx, dep, hsh)
+            counts[i] = mask.sum()
+        counts_h.copy_(counts, non_blocking=True)
+
+    for _ in range(2):
+        one()
+    torch.cuda.synchronize(dev)
+    ts = []
+    for _ in range(max(args.e2e_steps, 1)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        one()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ts.append(e0.elapsed_time(e1))
+    ms = sum(ts) / len(ts)
+    return {"value": pipe_hw * len(sc.cameras) / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": ms, "api": "epcq.NeuralPoints.pts2plane + "
+            "render_image_hashtable_topk per view, xyz and cameras copied from pinned host memory each step, "
+            "per-view emitted-sample counts read back"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from hashpoint import synth
+    sc = synth.make_shapes(n_views=1, with_feat=False)
+    for _ in range(args.warmup):
+        cpu_baseline(n_views=1, scene=sc)
+    vals = [cpu_baseline(n_views=1, scene=sc) for _ in range(args.steps)]
+    value = sum(v["value"] for v in vals) / len(vals)
+    base = dict(vals[-1])
+    base["value"] = value
+    base["sample"] = "per step " + base["sample"]
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 640000 / value * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no public dataset)",
+        "config": config_dict(args, {"views_per_step": 1, "rays_per_step": 640000}), "impl": "reference",
+        "cpu_baseline": base,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -10,27 +10,30 @@
 //                     exact rounding, atomic slot within the pixel's bucket
 //   k_block_sums      per-block totals of the H*W counts
 //   k_scan_hash       exclusive scan -> hash_table (start, count) / (-1, -1)
-//   k_scatter         every point to start + slot; -1 into the off-image tail
-//   k_sort_small      buckets of 2..16 entries sorted in registers by a
-//                     bitonic network (thread per pixel)
-//   k_sort_deep       larger buckets: one CTA at a time, bitonic sort in
-//                     shared memory (<= 2048 entries) or in place in global memory
+//   k_scatter         every point to start + slot of a scratch copy (id, depth,
+//                     pixel); -1 into the off-image tail of the outputs
+//   k_order           one thread per bucket entry: its rank among its bucket's
+//                     entries gives its final position (buckets <= 2048)
+//   k_sort_huge       buckets above 2048 entries: one CTA each, bitonic sort
+//                     in place in global memory
 //
-// The atomic slots make the order inside a bucket arbitrary; the per-bucket
-// sort restores the reference's order: ascending point id (the stable sort's
-// order) when sort == 0, (depth, id) when sort != 0 (its stable bubble sort).
+// The atomic slots make the order inside a bucket arbitrary; ranking restores
+// the reference's order: ascending point id (the stable sort's order) when
+// sort == 0, (depth, id) when sort != 0 (its stable bubble sort).  Rank
+// sorting costs sum(c^2) comparisons over buckets of c entries, which for
+// point clouds (a few to a few hundred points per pixel) is far cheaper than
+// a serial sort per bucket, and every thread does useful work.
 #include <cstdio>
 
 #include "hp_common.cuh"
 
 namespace hp {
 
-constexpr int kSmallBucket = 16;
+constexpr int kRankMax = 2048;                   // largest bucket ordered by ranking
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;                    // counts per thread in the scan
 constexpr int kScanTile = kScanThreads * kScanItems;
-constexpr int kDeepSmem = 2048;                  // entries a CTA sorts in shared memory
-constexpr int kDeepThreads = 256;
+constexpr int kHugeThreads = 512;
 
 // Bucket sort key: the point id (sort == 0) or (depth, id) with depth mapped to
 // an order-preserving integer (-0.0 folded onto +0.0 as float comparison does).
@@ -168,15 +171,17 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_hash(const int* __restric
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_scatter(int n, int hw, const int2* __restrict__ pid_slot,
                                                  const float* __restrict__ depth, const int2* __restrict__ hash,
-                                                 const int* __restrict__ scalars, int* __restrict__ out_idx,
-                                                 float* __restrict__ out_depth) {
+                                                 const int* __restrict__ scalars, int* __restrict__ tmp_id,
+                                                 float* __restrict__ tmp_depth, int* __restrict__ tmp_pid,
+                                                 int* __restrict__ out_idx, float* __restrict__ out_depth) {
   const int n_in = scalars[0];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int2 ps = pid_slot[i];
     if (ps.x < hw) {
       const int pos = hash[ps.x].x + ps.y;
-      out_idx[pos] = i;
-      out_depth[pos] = depth[i];
+      tmp_id[pos] = i;
+      tmp_depth[pos] = depth[i];
+      tmp_pid[pos] = ps.x;
     }
     if (i >= n_in) {
       out_idx[i] = -1;
@@ -188,107 +193,53 @@ __global__ void __launch_bounds__(256) k_scatter(int n, int hw, const int2* __re
 // ---------------------------------------------------------------------------
 // per-bucket order
 // ---------------------------------------------------------------------------
-// Keys are (hi, lo): hi = order-preserving depth bits (or 0 when ordering by
-// id alone), lo = point id, or -- when `gather` is set -- the entry's index in
-// the caller's input, so depth ties keep the input order and the id is read
-// back from gather[lo].  Depth travels with the key.
+// Entry keys are (hi, lo): hi = order-preserving depth bits (0 when ordering by
+// id alone), lo = the point id, or -- for hp_scatter_hashtable, whose input
+// order inside a run must survive depth ties -- the entry's input position.
 struct BucketOrder {
   int by_depth;
-  const int* gather;  // hp_scatter_hashtable's point_idx input, or nullptr
+  int by_position;  // tie-break on the input position instead of the id
 };
 
-__device__ __forceinline__ unsigned long long entry_key(const BucketOrder& bo, int id_or_pos, float depth) {
-  return sort_key(id_or_pos, depth, bo.by_depth);
+__device__ __forceinline__ unsigned long long entry_key(const BucketOrder& bo, int id, float depth, int pos) {
+  return sort_key(bo.by_position ? pos : id, depth, bo.by_depth);
 }
 
-template <int N>
-__device__ __forceinline__ void network_sort(unsigned long long (&key)[N], float (&dep)[N]) {
-  // bitonic sorting network, ascending; all indices compile-time -> registers
-#pragma unroll
-  for (int k = 2; k <= N; k <<= 1) {
-#pragma unroll
-    for (int j = k >> 1; j > 0; j >>= 1) {
-#pragma unroll
-      for (int i = 0; i < N; i++) {
-        const int l = i ^ j;
-        if (l > i) {
-          const bool up = (i & k) == 0;
-          const bool swap = up ? (key[i] > key[l]) : (key[i] < key[l]);
-          if (swap) {
-            const unsigned long long tk = key[i];
-            key[i] = key[l];
-            key[l] = tk;
-            const float td = dep[i];
-            dep[i] = dep[l];
-            dep[l] = td;
-          }
-        }
-      }
+// One thread per entry j < n_in of the scratch copy: rank among the entries of
+// its bucket -> final position.  Buckets of one entry are copied; buckets above
+// kRankMax are left to k_sort_huge.
+__global__ void __launch_bounds__(256) k_order(const int* __restrict__ in_id, const float* __restrict__ in_depth,
+                                               const int* __restrict__ in_pid, const int2* __restrict__ hash, int hw,
+                                               const int* __restrict__ scalars, int n_fixed,
+                                               int* __restrict__ out_idx, float* __restrict__ out_depth,
+                                               BucketOrder bo) {
+  const int n_in = n_fixed >= 0 ? n_fixed : scalars[0];
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_in; j += gridDim.x * blockDim.x) {
+    const int p = in_pid[j];
+    if (p < 0 || p >= hw) continue;
+    const int2 h = hash[p];
+    const int id = in_id[j];
+    const float d = in_depth[j];
+    if (h.y > kRankMax) continue;
+    int pos = h.x;
+    if (h.y > 1) {
+      const unsigned long long kj = entry_key(bo, id, d, j);
+      int rank = 0;
+      for (int q = h.x; q < h.x + h.y; q++) rank += entry_key(bo, __ldg(in_id + q), __ldg(in_depth + q), q) < kj;
+      pos += rank;
     }
+    out_idx[pos] = id;
+    out_depth[pos] = d;
   }
 }
 
-__device__ __forceinline__ int key_id(const BucketOrder& bo, unsigned long long key) {
-  const int lo = (int)(unsigned)(key & 0xffffffffull);
-  return bo.gather ? bo.gather[lo] : lo;
-}
-
-// Sort the c (<= N) entries at idx/dep; `first` is their absolute position.
-template <int N>
-__device__ __forceinline__ void sort_bucket_regs(const BucketOrder& bo, int* __restrict__ idx,
-                                                 float* __restrict__ dep_arr, int c, int first) {
-  unsigned long long key[N];
-  float dep[N];
-#pragma unroll
-  for (int i = 0; i < N; i++) {
-    if (i < c) {
-      dep[i] = dep_arr[i];
-      key[i] = entry_key(bo, bo.gather ? first + i : idx[i], dep[i]);
-    } else {
-      dep[i] = 0.0f;
-      key[i] = ~0ull;
-    }
-  }
-  network_sort<N>(key, dep);
-#pragma unroll
-  for (int i = 0; i < N; i++)
-    if (i < c) {
-      idx[i] = key_id(bo, key[i]);
-      dep_arr[i] = dep[i];
-    }
-}
-
-__global__ void __launch_bounds__(256) k_sort_small(int hw, const int2* __restrict__ hash, int* __restrict__ out_idx,
-                                                    float* __restrict__ out_depth, BucketOrder bo) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= hw) return;
-  const int2 h = hash[p];
-  const int c = h.y;
-  if (c < 2 || c > kSmallBucket) return;
-  int* idx = out_idx + h.x;
-  float* dep = out_depth + h.x;
-  if (c <= 2) {
-    sort_bucket_regs<2>(bo, idx, dep, c, h.x);
-  } else if (c <= 4) {
-    sort_bucket_regs<4>(bo, idx, dep, c, h.x);
-  } else if (c <= 8) {
-    sort_bucket_regs<8>(bo, idx, dep, c, h.x);
-  } else {
-    sort_bucket_regs<16>(bo, idx, dep, c, h.x);
-  }
-}
-
-// Large buckets: each CTA scans a contiguous range of pixels kDeepThreads at a
-// time, queues the deep ones in shared memory and sorts them one by one.
-// Up to kDeepSmem entries are sorted in shared memory (keys + depth); larger
-// buckets are sorted in place in global memory by a bitonic network in its
-// "flip" form (every comparator is ascending towards the larger index, so
-// positions past the bucket act as +inf and are never touched), with keys
-// for the gather mode kept in a per-bucket scratch of the sort itself: the
-// output idx array holds the input positions until the final gather.
+// Compare-exchange of positions i < l (ascending) in a bucket of c entries;
+// positions >= c act as +inf and are never touched (the "flip" bitonic
+// variant compares only towards the larger index, ascending).  While sorting,
+// idx holds input positions in the by_position mode.
 __device__ __forceinline__ void cx_global(const BucketOrder& bo, int* idx, float* dep, int i, int l, int c) {
   if (l >= c) return;
-  const unsigned long long ki = entry_key(bo, idx[i], dep[i]), kl = entry_key(bo, idx[l], dep[l]);
+  const unsigned long long ki = sort_key(idx[i], dep[i], bo.by_depth), kl = sort_key(idx[l], dep[l], bo.by_depth);
   if (ki > kl) {
     const int t = idx[i];
     idx[i] = idx[l];
@@ -299,12 +250,16 @@ __device__ __forceinline__ void cx_global(const BucketOrder& bo, int* idx, float
   }
 }
 
-__global__ void __launch_bounds__(kDeepThreads) k_sort_deep(int hw, const int2* __restrict__ hash,
+// Buckets above kRankMax entries (pathological inputs): each CTA scans a
+// contiguous range of pixels blockDim at a time, queues the huge ones in shared
+// memory, and sorts each in place in global memory after copying it from the
+// scratch arrays (in_id / in_depth, indexed by position).
+__global__ void __launch_bounds__(kHugeThreads) k_sort_huge(int hw, const int* __restrict__ in_id,
+                                                            const float* __restrict__ in_depth,
+                                                            const int2* __restrict__ hash,
                                                             int* __restrict__ out_idx, float* __restrict__ out_depth,
                                                             BucketOrder bo) {
-  __shared__ unsigned long long sk[kDeepSmem];
-  __shared__ float sd[kDeepSmem];
-  __shared__ int queue[kDeepThreads];
+  __shared__ int queue[kHugeThreads];
   __shared__ int qn;
   const int per = (hw + gridDim.x - 1) / gridDim.x;
   const int lo = blockIdx.x * per, hi = min(hw, lo + per);
@@ -312,7 +267,7 @@ __global__ void __launch_bounds__(kDeepThreads) k_sort_deep(int hw, const int2* 
     if (threadIdx.x == 0) qn = 0;
     __syncthreads();
     const int p = base + threadIdx.x;
-    if (p < hi && hash[p].y > kSmallBucket) queue[atomicAdd(&qn, 1)] = p;
+    if (p < hi && hash[p].y > kRankMax) queue[atomicAdd(&qn, 1)] = p;
     __syncthreads();
     const int nq = qn;
     for (int q = 0; q < nq; q++) {
@@ -320,66 +275,31 @@ __global__ void __launch_bounds__(kDeepThreads) k_sort_deep(int hw, const int2* 
       const int c = h.y;
       int* idx = out_idx + h.x;
       float* dep = out_depth + h.x;
+      for (int i = threadIdx.x; i < c; i += blockDim.x) {
+        idx[i] = bo.by_position ? h.x + i : in_id[h.x + i];
+        dep[i] = in_depth[h.x + i];
+      }
+      __syncthreads();
       int npow = 1;
       while (npow < c) npow <<= 1;
-      if (c <= kDeepSmem) {
-        for (int i = threadIdx.x; i < npow; i += blockDim.x) {
-          if (i < c) {
-            sd[i] = dep[i];
-            sk[i] = entry_key(bo, bo.gather ? h.x + i : idx[i], sd[i]);
-          } else {
-            sk[i] = ~0ull;
-            sd[i] = 0.0f;
-          }
+      for (int k = 2; k <= npow; k <<= 1) {
+        for (int i = threadIdx.x; i < npow / 2; i += blockDim.x) {
+          const int blk = i / (k >> 1), off = i % (k >> 1);
+          const int a = blk * k + off, b = blk * k + k - 1 - off;
+          if (a < c) cx_global(bo, idx, dep, a, b, c);
         }
         __syncthreads();
-        for (int k = 2; k <= npow; k <<= 1) {
-          for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < npow; i += blockDim.x) {
-              const int l = i ^ j;
-              if (l > i) {
-                const bool up = (i & k) == 0;
-                const unsigned long long a = sk[i], b = sk[l];
-                if (up ? a > b : a < b) {
-                  sk[i] = b;
-                  sk[l] = a;
-                  const float t = sd[i];
-                  sd[i] = sd[l];
-                  sd[l] = t;
-                }
-              }
-            }
-            __syncthreads();
-          }
-        }
-        for (int i = threadIdx.x; i < c; i += blockDim.x) {
-          idx[i] = key_id(bo, sk[i]);
-          dep[i] = sd[i];
-        }
-      } else {
-        // positions stand in for ids while sorting in the gather mode
-        if (bo.gather)
-          for (int i = threadIdx.x; i < c; i += blockDim.x) idx[i] = h.x + i;
-        __syncthreads();
-        for (int k = 2; k <= npow; k <<= 1) {
+        for (int j = k >> 2; j > 0; j >>= 1) {
           for (int i = threadIdx.x; i < npow / 2; i += blockDim.x) {
-            const int blk = i / (k >> 1), off = i % (k >> 1);
-            const int a = blk * k + off, b = blk * k + k - 1 - off;
-            if (a < c) cx_global(bo, idx, dep, a, b, c);
+            const int blk = i / j, off = i % j;
+            const int a = blk * 2 * j + off;
+            if (a < c) cx_global(bo, idx, dep, a, a + j, c);
           }
           __syncthreads();
-          for (int j = k >> 2; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < npow / 2; i += blockDim.x) {
-              const int blk = i / j, off = i % j;
-              const int a = blk * 2 * j + off;
-              if (a < c) cx_global(bo, idx, dep, a, a + j, c);
-            }
-            __syncthreads();
-          }
         }
-        if (bo.gather)
-          for (int i = threadIdx.x; i < c; i += blockDim.x) idx[i] = bo.gather[idx[i]];
       }
+      if (bo.by_position)
+        for (int i = threadIdx.x; i < c; i += blockDim.x) idx[i] = in_id[idx[i]];
       __syncthreads();
     }
     __syncthreads();
@@ -416,7 +336,7 @@ __global__ void __launch_bounds__(256) k_runs(const int* __restrict__ point_idx,
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct BuildLayout {
-  size_t counts, block_sums, pid_slot, depth, scalars, total;
+  size_t counts, block_sums, pid_slot, depth, tmp_id, tmp_depth, tmp_pid, scalars, total;
 };
 
 static BuildLayout build_layout(int64_t n, int64_t hw) {
@@ -431,6 +351,12 @@ static BuildLayout build_layout(int64_t n, int64_t hw) {
   o += align256(sizeof(int2) * (size_t)(n > 0 ? n : 1));
   L.depth = o;
   o += align256(sizeof(float) * (size_t)(n > 0 ? n : 1));
+  L.tmp_id = o;
+  o += align256(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  L.tmp_depth = o;
+  o += align256(sizeof(float) * (size_t)(n > 0 ? n : 1));
+  L.tmp_pid = o;
+  o += align256(sizeof(int) * (size_t)(n > 0 ? n : 1));
   L.scalars = o;
   o += 256;
   L.total = o;
@@ -444,14 +370,19 @@ static int grid_for(int64_t n, int threads) {
   return (int)(g > 0 ? g : 1);
 }
 
-// Bucket-order fix-up shared by hp_pts2plane and hp_scatter_hashtable.
-static int32_t launch_bucket_sort(int hw, const int2* hash, int* out_idx, float* out_depth, BucketOrder bo,
-                                  cudaStream_t st) {
-  k_sort_small<<<(hw + 255) / 256, 256, 0, st>>>(hw, hash, out_idx, out_depth, bo);
-  if (int32_t rc = check_launch("k_sort_small")) return rc;
-  const int blocks = hw < 148 * 4 * kDeepThreads ? (hw + kDeepThreads - 1) / kDeepThreads : 148 * 4;
-  k_sort_deep<<<blocks, kDeepThreads, 0, st>>>(hw, hash, out_idx, out_depth, bo);
-  return check_launch("k_sort_deep");
+// Bucket order shared by hp_pts2plane (entries in scratch arrays, count on
+// the device) and hp_scatter_hashtable (entries in the caller's sorted input).
+static int32_t launch_order(int hw, int n_fixed, int n_grid, const int* in_id, const float* in_depth, const int* in_pid,
+                            const int2* hash, const int* scalars, int* out_idx, float* out_depth, BucketOrder bo,
+                            cudaStream_t st) {
+  if (n_grid > 0) {
+    k_order<<<grid_for(n_grid, 256), 256, 0, st>>>(in_id, in_depth, in_pid, hash, hw, scalars, n_fixed, out_idx,
+                                                    out_depth, bo);
+    if (int32_t rc = check_launch("k_order")) return rc;
+  }
+  const int blocks = (hw + kHugeThreads - 1) / kHugeThreads < 148 * 2 ? (hw + kHugeThreads - 1) / kHugeThreads : 148 * 2;
+  k_sort_huge<<<blocks, kHugeThreads, 0, st>>>(hw, in_id, in_depth, hash, out_idx, out_depth, bo);
+  return check_launch("k_sort_huge");
 }
 
 }  // namespace hp
@@ -496,6 +427,9 @@ extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_cam
   int* block_sums = (int*)(ws + L.block_sums);
   int2* pid_slot = (int2*)(ws + L.pid_slot);
   float* depth = (float*)(ws + L.depth);
+  int* tmp_id = (int*)(ws + L.tmp_id);
+  float* tmp_depth = (float*)(ws + L.tmp_depth);
+  int* tmp_pid = (int*)(ws + L.tmp_pid);
   int* scalars = (int*)(ws + L.scalars);
   int2* hash = (int2*)hash_table;
   const int n = (int)n_points;
@@ -516,11 +450,12 @@ extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_cam
   k_scan_hash<<<nblk, kScanThreads, 0, st>>>(counts, (int)hw, block_sums, hash, scalars);
   if (int32_t rc = check_launch("k_scan_hash")) return rc;
   if (n > 0) {
-    k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, (int)hw, pid_slot, depth, hash, scalars, sorted_point_idx,
-                                                sorted_depth);
+    k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, (int)hw, pid_slot, depth, hash, scalars, tmp_id, tmp_depth, tmp_pid,
+                                                sorted_point_idx, sorted_depth);
     if (int32_t rc = check_launch("k_scatter")) return rc;
   }
-  return launch_bucket_sort((int)hw, hash, sorted_point_idx, sorted_depth, BucketOrder{sort != 0, nullptr}, st);
+  return launch_order((int)hw, -1, n, tmp_id, tmp_depth, tmp_pid, hash, scalars, sorted_point_idx, sorted_depth,
+                      BucketOrder{sort != 0, 0}, st);
 }
 
 extern "C" int32_t hp_scatter_hashtable(const int32_t* point_idx, const int32_t* point2img, const float* depth,
@@ -546,5 +481,7 @@ extern "C" int32_t hp_scatter_hashtable(const int32_t* point_idx, const int32_t*
     if (int32_t rc = check_launch("k_runs")) return rc;
   }
   if (!sort) return HP_OK;
-  return launch_bucket_sort(hw, hash, sorted_point_idx, sorted_depth, BucketOrder{1, point_idx}, st);
+  // depth order inside each run, ties kept in input order
+  return launch_order(hw, (int)n, (int)n, point_idx, depth, point2img, hash, nullptr, sorted_point_idx, sorted_depth,
+                      BucketOrder{1, 1}, st);
 }

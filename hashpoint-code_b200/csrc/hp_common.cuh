@@ -16,13 +16,15 @@
 
 // Point counts above which torch's cuBLAS GEMMs of the reference projection
 // (epcq/epcq.py:253 world->camera, :261 camera->image) used a fused
-// multiply-add chain on B200; at or below them each product was rounded
-// separately.  Established by diffing torch outputs against both forms.
+// multiply-add chain on B200 (torch 2.11, cuBLAS 12.8); at or below them each
+// product was rounded separately.  Established by diffing torch outputs against
+// both forms for every N in 2..2100 and every 8th N in 200000..260000; N = 1
+// matched neither form for the world->camera product.
 #ifndef HP_WORLD_FUSED_ABOVE
-#define HP_WORLD_FUSED_ABOVE 1000
+#define HP_WORLD_FUSED_ABOVE 1536
 #endif
 #ifndef HP_IMAGE_FUSED_ABOVE
-#define HP_IMAGE_FUSED_ABOVE 100000
+#define HP_IMAGE_FUSED_ABOVE 233023
 #endif
 
 namespace hp {

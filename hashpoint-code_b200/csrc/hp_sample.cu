@@ -6,13 +6,15 @@
 // per ray, one lane per window cell, a 128-bin shared-memory histogram built
 // with float atomics and a serial walk on lane 0) and then
 // quick_search_nearby_pc (:10-81, one thread per (ray, sample slot) re-walking
-// the window).  Here one thread owns one ray end to end and writes every
-// output element of that ray exactly once:
+// the window).  Here a CTA owns a 4x32 pixel tile: it stages the points of
+// the tile's window halo (clamped to the image) into shared memory once as
+// float4 (x, y, z, id) with coalesced gathers, then one thread owns one ray
+// end to end and writes every output element of that ray exactly once:
 //
 //   pass A  kept candidates (ray distance < radius, at most 48 per window cell,
 //           cells row-major and clamped, bucket order) -> tmin, tmax
 //   pass B  the same candidates binned by int((t - tmin) / t_intvl); instead of
-//           a 128-bin histogram the thread keeps the 8 smallest distinct bins
+//           a 128-bin histogram the thread keeps the 4 smallest distinct bins
 //           (count, distance sum) in registers -- exactly the bins the walk
 //           reaches first -- and re-collects further bins only if the walk
 //           goes past them
@@ -21,7 +23,17 @@
 //           stop when T < 1e-3 or S samples are out
 //   ball    per emitted sample, the reference's 8-entry id buffer over the
 //           whole window (including its quirk that, while the buffer fills, the
-//           tracked "farthest" entry is the nearest one)
+//           tracked "farthest" entry is the nearest one).  Candidates whose
+//           position along the ray is further than radius (+ a rounding
+//           margin orders of magnitude above float error) from the sample are
+//           skipped before the distance is computed: they cannot be within
+//           the radius, so the buffer sees exactly the same sequence.
+//
+// Each pass walks the ray's window as one flat candidate sequence, so the
+// lanes of a warp (32 neighbouring pixels, whose windows overlap) run loops of
+// similar length instead of diverging on every cell's bucket size.  Tiles
+// whose halo holds more than kStageCap points read candidates straight from
+// global memory through the same code.
 //
 // Bin sums are accumulated in window-cell then bucket order; the reference
 // adds them with shared-memory atomics in an unspecified order, so a bin's
@@ -33,7 +45,12 @@ namespace hp {
 
 constexpr int kTileW = 32;   // pixels of one image row per warp
 constexpr int kTileH = 4;    // rows per block
-constexpr int kBinList = 8;  // distinct t-bins collected per candidate pass
+constexpr int kThreads = kTileW * kTileH;
+constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
+constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
+constexpr int kStageCap = 2048;  // staged points per tile (32 KB)
+constexpr int kBinList = 4;      // distinct t-bins collected per candidate pass
+constexpr int kTeReg = 4;        // emitted sample depths kept in registers
 
 struct SampleArgs {
   const float* __restrict__ xyz;
@@ -49,74 +66,116 @@ struct SampleArgs {
   uint8_t* __restrict__ mask;
 };
 
-// Kept candidates in the reference's order: window cells 0..ncell-1, bucket
-// order, at most kKeptPerCell kept per cell; f(t, dist) for each.
-template <typename F>
-__device__ __forceinline__ void for_each_kept(const SampleArgs& a, const Ray& r, int v, int u, int ncell, F&& f) {
-  const int H = a.cam.height, W = a.cam.width, k = a.opt.k;
-  for (int l = 0; l < ncell; l++) {
-    int vv, uu;
-    window_cell(v, u, k, H, W, l, vv, uu);
-    const int2 h = __ldg(a.hash + (size_t)vv * W + uu);
-    if (h.y <= 0 || h.x < 0) continue;
-    int nk = 0;
-    const int end = min(h.x + min(h.y, a.n_sorted), a.n_sorted);
-    for (int j = h.x; j < end && nk < kKeptPerCell; j++) {
-      const int id = __ldg(a.sidx + j);
-      if ((unsigned)id >= (unsigned)a.n_points) continue;
-      const float4 p = load_point(a.xyz, id);
-      float t, dist;
-      intersect(r, p.x, p.y, p.z, t, dist);
-      if (dist < a.opt.radius) {
-        nk++;
-        f(t, dist);
-      }
-    }
-  }
+struct Stage {
+  float4 cand[kStageCap];  // x, y, z, id (as int bits; -1 = invalid id)
+  int off[kHaloMax + 1];   // staged offset of each halo cell, exclusive prefix
+  int start[kHaloMax];     // the cell's first index in sorted_point_idx
+  int warp_tot[kThreads / 32];
+};
+
+// Clipped bucket range of a hash entry: [x, x + count) within [0, n_sorted).
+__device__ __forceinline__ int2 bucket_range(int2 h, int n_sorted) {
+  if (h.x < 0 || h.y <= 0 || h.x >= n_sorted) return make_int2(0, 0);
+  return make_int2(h.x, h.x + min(h.y, n_sorted - h.x));
 }
 
-// Every window point (all k*k cells, no cap), f(id, point).
-template <typename F>
-__device__ __forceinline__ void for_each_window_point(const SampleArgs& a, int v, int u, int k2, F&& f) {
-  const int H = a.cam.height, W = a.cam.width, k = a.opt.k;
-  for (int l = 0; l < k2; l++) {
-    int vv, uu;
-    window_cell(v, u, k, H, W, l, vv, uu);
-    const int2 h = __ldg(a.hash + (size_t)vv * W + uu);
-    if (h.y < 0 || h.x < 0) continue;
-    const int end = min(h.x + min(h.y, a.n_sorted), a.n_sorted);
-    for (int j = h.x; j < end; j++) {
-      const int id = __ldg(a.sidx + j);
-      if ((unsigned)id >= (unsigned)a.n_points) continue;
-      f(id, load_point(a.xyz, id));
-    }
+// Candidates from the tile's shared-memory stage.
+struct SrcStaged {
+  const Stage* st;
+  int rv0, ru0, nu;
+  __device__ __forceinline__ int2 range(const SampleArgs&, int vv, int uu) const {
+    const int c = (vv - rv0) * nu + (uu - ru0);
+    return make_int2(st->off[c], st->off[c + 1]);
   }
+  __device__ __forceinline__ float4 fetch(const SampleArgs&, int i) const { return st->cand[i]; }
+};
+
+// Candidates straight from global memory (tiles whose halo overflows the stage).
+struct SrcGlobal {
+  __device__ __forceinline__ int2 range(const SampleArgs& a, int vv, int uu) const {
+    return bucket_range(__ldg(a.hash + (size_t)vv * a.cam.width + uu), a.n_sorted);
+  }
+  __device__ __forceinline__ float4 fetch(const SampleArgs& a, int j) const {
+    const int id = __ldg(a.sidx + j);
+    if ((unsigned)id >= (unsigned)a.n_points) return make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    const float4 p = load_point(a.xyz, id);
+    return make_float4(p.x, p.y, p.z, __int_as_float(id));
+  }
+};
+
+// A flat walk over the candidates of window cells 0..ncell-1 (row-major,
+// clamped), at most `cap` accepted per cell (the caller counts acceptances in nk).
+struct Walk {
+  int l, j, end, nk;
+};
+
+template <class Src>
+__device__ __forceinline__ bool walk_next(Walk& w, const Src& src, const SampleArgs& a, int v, int u, int ncell,
+                                          int cap) {
+  while (w.j >= w.end || w.nk >= cap) {
+    if (++w.l >= ncell) return false;
+    int vv, uu;
+    window_cell(v, u, a.opt.k, a.cam.height, a.cam.width, w.l, vv, uu);
+    const int2 r = src.range(a, vv, uu);
+    w.j = r.x;
+    w.end = r.y;
+    w.nk = 0;
+  }
+  return true;
 }
 
-__global__ void __launch_bounds__(kTileW* kTileH) k_quick_sampling(SampleArgs a) {
-  const int u = blockIdx.x * kTileW + (threadIdx.x & 31);
-  const int v = blockIdx.y * kTileH + (threadIdx.x >> 5);
-  const int W = a.cam.width, H = a.cam.height;
-  if (u >= W || v >= H) return;
+// Fill n elements from p with v using 16-byte stores where aligned.
+template <typename T>
+__device__ __forceinline__ void fill_run(T* p, int n, T v) {
+  constexpr int kVec = 16 / sizeof(T);
+  int i = 0;
+  while (i < n && (((uintptr_t)(p + i)) & 15) != 0) p[i++] = v;
+  if (i + kVec <= n) {
+    T vv[kVec];
+#pragma unroll
+    for (int q = 0; q < kVec; q++) vv[q] = v;
+    const int4 pack = *reinterpret_cast<const int4*>(vv);
+    for (; i + kVec <= n; i += kVec) *reinterpret_cast<int4*>(p + i) = pack;
+  }
+  for (; i < n; i++) p[i] = v;
+}
+
+template <class Src>
+__device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, int v, int u) {
+  const int W = a.cam.width;
   const int ray = v * W + u;
   const int S = a.opt.S, P = a.opt.P, k = a.opt.k, k2 = k * k;
   const int ncell = k2 < kLaneCells ? k2 : kLaneCells;
+  const float radius = a.opt.radius;
 
   Ray r;
   make_ray(a.cam.c2w, a.cam.fx, a.cam.fy, a.cam.cx, a.cam.cy, u, v, r);
 
   // pass A: tmin / tmax over the kept candidates (epcq_render_topk.cu:132-161)
   float tmin = 1e3f, tmax = -1e3f;
-  for_each_kept(a, r, v, u, ncell, [&](float t, float) {
-    if (tmin > t) tmin = t;
-    if (tmax < t) tmax = t;
-  });
+  {
+    Walk w{-1, 0, 0, 0};
+    while (walk_next(w, src, a, v, u, ncell, kKeptPerCell)) {
+      const float4 p = src.fetch(a, w.j++);
+      if (__float_as_int(p.w) < 0) continue;
+      float t, dist;
+      intersect(r, p.x, p.y, p.z, t, dist);
+      if (dist < radius) {
+        w.nk++;
+        if (tmin > t) tmin = t;
+        if (tmax < t) tmax = t;
+      }
+    }
+  }
 
   float* o_xyz = a.sp_xyz + (size_t)ray * S * 3;
   float* o_t = a.sp_t + (size_t)ray * S;
   uint8_t* o_m = a.mask + (size_t)ray * S;
   int* o_idx = a.pc_idx + (size_t)ray * S * P;
   int emitted = 0;
+  float te[kTeReg];
+#pragma unroll
+  for (int q = 0; q < kTeReg; q++) te[q] = 0.0f;
 
   if (!(tmin > tmax)) {
     float transmit = 1.0f;
@@ -128,9 +187,16 @@ __global__ void __launch_bounds__(kTileW* kTileH) k_quick_sampling(SampleArgs a)
 #pragma unroll
       for (int q = 0; q < kBinList; q++) lb[q] = 0x7fffffff, lc[q] = 0, ls[q] = 0.0f;
       int m = 0, cut = kBins;
-      for_each_kept(a, r, v, u, ncell, [&](float t, float dist) {
+      Walk w{-1, 0, 0, 0};
+      while (walk_next(w, src, a, v, u, ncell, kKeptPerCell)) {
+        const float4 p = src.fetch(a, w.j++);
+        if (__float_as_int(p.w) < 0) continue;
+        float t, dist;
+        intersect(r, p.x, p.y, p.z, t, dist);
+        if (!(dist < radius)) continue;
+        w.nk++;
         const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
-        if (b < lo || b >= cut) return;
+        if (b < lo || b >= cut) continue;
         bool found = false;
 #pragma unroll
         for (int q = 0; q < kBinList; q++)
@@ -139,10 +205,10 @@ __global__ void __launch_bounds__(kTileW* kTileH) k_quick_sampling(SampleArgs a)
             ls[q] = __fadd_rn(ls[q], dist);
             found = true;
           }
-        if (found) return;
+        if (found) continue;
         if (m == kBinList && b > lb[kBinList - 1]) {
           cut = b;
-          return;
+          continue;
         }
         int pos = 0;
 #pragma unroll
@@ -161,7 +227,7 @@ __global__ void __launch_bounds__(kTileW* kTileH) k_quick_sampling(SampleArgs a)
           }
         }
         m = m < kBinList ? m + 1 : kBinList;
-      });
+      }
       // primary-surface walk (epcq_render_topk.cu:181-204)
       bool done = false;
 #pragma unroll
@@ -182,6 +248,9 @@ __global__ void __launch_bounds__(kTileW* kTileH) k_quick_sampling(SampleArgs a)
           o_xyz[emitted * 3 + 2] = __fmaf_rn(t, r.d[2], r.o[2]);
           o_t[emitted] = t;
           o_m[emitted] = 1;
+#pragma unroll
+          for (int e = 0; e < kTeReg; e++)
+            if (e == emitted) te[e] = t;
           emitted++;
         }
         transmit = __fsub_rn(transmit, alpha);
@@ -192,17 +261,31 @@ __global__ void __launch_bounds__(kTileW* kTileH) k_quick_sampling(SampleArgs a)
   }
 
   // per-sample point selection (epcq_render_topk.cu:10-81)
+  const float omax = fmaxf(fabsf(r.o[0]), fmaxf(fabsf(r.o[1]), fabsf(r.o[2])));
   for (int s = 0; s < emitted; s++) {
-    const float sx = o_xyz[s * 3 + 0], sy = o_xyz[s * 3 + 1], sz = o_xyz[s * 3 + 2];
+    float ts = o_t[s];
+#pragma unroll
+    for (int e = 0; e < kTeReg; e++)
+      if (e == s) ts = te[e];
+    const float sx = __fmaf_rn(ts, r.d[0], r.o[0]), sy = __fmaf_rn(ts, r.d[1], r.o[1]),
+                sz = __fmaf_rn(ts, r.d[2], r.o[2]);
+    // |position along the ray - ts| beyond this cannot be within the radius
+    const float reach = radius * 1.001f + 1e-5f * (1.0f + fabsf(ts) + omax);
     float bd[kBallBuf];
     int bi[kBallBuf];
 #pragma unroll
     for (int q = 0; q < kBallBuf; q++) bd[q] = 0.0f, bi[q] = -1;
     int bsize = 0, maxi = 0;
     float maxd = 1e3f;
-    for_each_window_point(a, v, u, k2, [&](int id, float4 p) {
+    Walk w{-1, 0, 0, 0};
+    while (walk_next(w, src, a, v, u, k2, 0x7fffffff)) {
+      const float4 p = src.fetch(a, w.j++);
+      const int id = __float_as_int(p.w);
+      if (id < 0) continue;
+      const float along = dot3(p.x - r.o[0], p.y - r.o[1], p.z - r.o[2], r.d[0], r.d[1], r.d[2]);
+      if (fabsf(along - ts) > reach) continue;
       const float dist = norm3df(__fsub_rn(sx, p.x), __fsub_rn(sy, p.y), __fsub_rn(sz, p.z));
-      if (!(dist < a.opt.radius)) return;
+      if (!(dist < radius)) continue;
       if (bsize < kBallBuf) {
 #pragma unroll
         for (int q = 0; q < kBallBuf; q++)
@@ -224,24 +307,100 @@ __global__ void __launch_bounds__(kTileW* kTileH) k_quick_sampling(SampleArgs a)
             maxi = q;
           }
       }
-    });
+    }
     int* row = o_idx + (size_t)s * P;
 #pragma unroll
     for (int q = 0; q < kBallBuf; q++)
       if (q < P) row[q] = q < bsize ? bi[q] : -1;
-    for (int q = kBallBuf; q < P; q++) row[q] = -1;
+    if (P > kBallBuf) fill_run(row + kBallBuf, P - kBallBuf, -1);
   }
 
   // defaults for the slots nothing was emitted into
-  for (int s = emitted; s < S; s++) {
-    o_xyz[s * 3 + 0] = 0.0f;
-    o_xyz[s * 3 + 1] = 0.0f;
-    o_xyz[s * 3 + 2] = 0.0f;
-    o_t[s] = 0.0f;
-    o_m[s] = 0;
-    int* row = o_idx + (size_t)s * P;
-    for (int q = 0; q < P; q++) row[q] = -1;
+  if (emitted < S) {
+    fill_run(o_xyz + emitted * 3, (S - emitted) * 3, 0.0f);
+    fill_run(o_t + emitted, S - emitted, 0.0f);
+    fill_run(o_m + emitted, S - emitted, (uint8_t)0);
+    fill_run(o_idx + (size_t)emitted * P, (S - emitted) * P, -1);
   }
+}
+
+__global__ void __launch_bounds__(kThreads) k_quick_sampling(SampleArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Stage& st = *reinterpret_cast<Stage*>(smem_raw);
+  const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
+  const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
+  const int v0 = blockIdx.y * kTileH, u0 = blockIdx.x * kTileW;
+  const int rv0 = max(0, v0 - lo), rv1 = min(H - 1, v0 + kTileH - 1 + hi);
+  const int ru0 = max(0, u0 - lo), ru1 = min(W - 1, u0 + kTileW - 1 + hi);
+  const int nu = ru1 - ru0 + 1, ncells = (rv1 - rv0 + 1) * nu;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  // halo cell table: global start, clipped count, block-wide exclusive prefix
+  int cnt[kCellsPerThread];
+  int local = 0;
+#pragma unroll
+  for (int q = 0; q < kCellsPerThread; q++) {
+    const int c = tid * kCellsPerThread + q;
+    cnt[q] = 0;
+    if (c < ncells) {
+      const int vv = rv0 + c / nu, uu = ru0 + c % nu;
+      const int2 rg = bucket_range(__ldg(a.hash + (size_t)vv * W + uu), a.n_sorted);
+      st.start[c] = rg.x;
+      // capped so the prefix cannot overflow; a capped cell alone exceeds the stage
+      cnt[q] = min(rg.y - rg.x, kStageCap + 1);
+    }
+    local += cnt[q];
+  }
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) st.warp_tot[warp] = incl;
+  __syncthreads();
+  int base = incl - local;
+  for (int q = 0; q < warp; q++) base += st.warp_tot[q];
+  int total = 0;
+#pragma unroll
+  for (int q = 0; q < kThreads / 32; q++) total += st.warp_tot[q];
+#pragma unroll
+  for (int q = 0; q < kCellsPerThread; q++) {
+    const int c = tid * kCellsPerThread + q;
+    if (c < ncells) st.off[c] = base;
+    base += cnt[q];
+  }
+  if (tid == 0) st.off[ncells] = total;
+  __syncthreads();
+
+  const bool staged = total <= kStageCap;
+  if (staged) {
+    for (int i = tid; i < total; i += kThreads) {
+      int lo_c = 0, hi_c = ncells;  // off[lo_c] <= i < off[hi_c]
+      while (hi_c - lo_c > 1) {
+        const int mid = (lo_c + hi_c) >> 1;
+        if (st.off[mid] <= i)
+          lo_c = mid;
+        else
+          hi_c = mid;
+      }
+      const int id = __ldg(a.sidx + st.start[lo_c] + (i - st.off[lo_c]));
+      float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+      if ((unsigned)id < (unsigned)a.n_points) {
+        const float4 q = load_point(a.xyz, id);
+        p = make_float4(q.x, q.y, q.z, __int_as_float(id));
+      }
+      st.cand[i] = p;
+    }
+    __syncthreads();
+  }
+
+  const int u = u0 + lane, v = v0 + warp;
+  if (u >= W || v >= H) return;
+  if (staged)
+    sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v, u);
+  else
+    sample_ray(a, SrcGlobal{}, v, u);
 }
 
 __global__ void k_ray_directions(DevCamera cam, float* __restrict__ dirs) {
@@ -329,7 +488,7 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   a.sp_t = sp_t;
   a.mask = mask;
   const dim3 grid((cam->width + kTileW - 1) / kTileW, (cam->height + kTileH - 1) / kTileH);
-  k_quick_sampling<<<grid, kTileW * kTileH, 0, (cudaStream_t)stream>>>(a);
+  k_quick_sampling<<<grid, kThreads, sizeof(Stage), (cudaStream_t)stream>>>(a);
   return check_launch("k_quick_sampling");
 }
 

@@ -1,0 +1,86 @@
+"""Per-view pipeline over preallocated device buffers (the plain per-view launch).
+
+A ViewPipeline owns the workspace and the output buffers for one problem shape
+(point count, image size, options) and renders a view with two C-ABI calls:
+hp_pts2plane (projection + hash table) and hp_quick_sampling (search + sample +
+per-sample points).  Camera matrices are read from device memory, so many
+views can be described by a device-resident camera table and launched
+back-to-back without host synchronisation.
+"""
+import ctypes
+
+import torch
+
+from . import native
+from .ops import make_options
+
+_vp = ctypes.c_void_p
+
+
+class CameraTable:
+    """Device-resident cameras: c2w/w2c [V,4,4], K [V,3,3] float32, plus host intrinsics."""
+
+    def __init__(self, cams, device):
+        import numpy as np
+        self.n = len(cams)
+        self.c2w = torch.from_numpy(np.stack([c.c2w for c in cams]).astype(np.float32)).to(device).contiguous()
+        self.w2c = torch.from_numpy(np.stack([c.w2c for c in cams]).astype(np.float32)).to(device).contiguous()
+        self.K = torch.from_numpy(np.stack([c.K for c in cams]).astype(np.float32)).to(device).contiguous()
+        self.intr = [(c.fx, c.fy, c.cx, c.cy, c.width, c.height) for c in cams]
+
+    def struct(self, i):
+        fx, fy, cx, cy, W, H = self.intr[i]
+        cam = native.HpCamera()
+        cam.c2w = self.c2w.data_ptr() + i * 64
+        cam.w2c = self.w2c.data_ptr() + i * 64
+        cam.K = self.K.data_ptr() + i * 36
+        cam.fx, cam.fy, cam.cx, cam.cy = fx, fy, cx, cy
+        cam.width, cam.height = W, H
+        return cam
+
+
+class ViewPipeline:
+    """pts2plane + quick_sampling for a fixed (N, H, W, S, P), buffers allocated once."""
+
+    def __init__(self, n_points, height, width, options, device, sort=False):
+        self.n, self.H, self.W = int(n_points), int(height), int(width)
+        self.opt = make_options(options)
+        self.sort = int(bool(sort))
+        self.device = torch.device(device)
+        S, P = self.opt.num_sample_points_per_ray, self.opt.num_point_cloud_per_sp
+        L = native.lib()
+        self.ws_bytes = L.hp_pts2plane_workspace_size(self.n, self.H, self.W)
+        dev = self.device
+        self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=dev)
+        self.sidx = torch.empty(self.n, dtype=torch.int32, device=dev)
+        self.sdep = torch.empty(self.n, dtype=torch.float32, device=dev)
+        self.hash = torch.empty((self.H * self.W, 2), dtype=torch.int32, device=dev)
+        self.sp_xyz = torch.empty((self.H, self.W, S, 3), dtype=torch.float32, device=dev)
+        self.pc_idx = torch.empty((self.H, self.W, S, P), dtype=torch.int32, device=dev)
+        self.sp_t = torch.empty((self.H, self.W, S), dtype=torch.float32, device=dev)
+        self.mask = torch.empty((self.H, self.W, S), dtype=torch.bool, device=dev)
+
+    def build(self, xyz, cam, stream):
+        rc = native.lib().hp_pts2plane(_vp(xyz.data_ptr()), self.n, ctypes.byref(cam), self.sort,
+                                       _vp(self.sidx.data_ptr()), _vp(self.sdep.data_ptr()),
+                                       _vp(self.hash.data_ptr()), _vp(self.ws.data_ptr()), self.ws_bytes,
+                                       _vp(stream.cuda_stream))
+        native.check(rc, "hp_pts2plane")
+
+    def sample(self, xyz, cam, stream):
+        rc = native.lib().hp_quick_sampling(_vp(xyz.data_ptr()), self.n, ctypes.byref(cam), ctypes.byref(self.opt),
+                                            _vp(self.sidx.data_ptr()), self.n, _vp(self.hash.data_ptr()),
+                                            _vp(self.sp_xyz.data_ptr()), _vp(self.pc_idx.data_ptr()),
+                                            _vp(self.sp_t.data_ptr()), _vp(self.mask.data_ptr()),
+                                            _vp(stream.cuda_stream))
+        native.check(rc, "hp_quick_sampling")
+
+    def render(self, xyz, cam, stream=None):
+        stream = stream or torch.cuda.current_stream(self.device)
+        self.build(xyz, cam, stream)
+        self.sample(xyz, cam, stream)
+        return self.sp_xyz, self.pc_idx, self.sp_t, self.mask
+
+    # kernels each render() launches (hp_pts2plane: project/count, block sums,
+    # scan, scatter, small-bucket sort, deep-bucket sort; hp_quick_sampling: 1)
+    KERNELS_PER_VIEW = 7

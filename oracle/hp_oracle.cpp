@@ -22,10 +22,10 @@
 // Point counts above which cuBLAS used an FMA chain for the world->camera and
 // the camera->image 3x3 @ 3xN GEMMs of epcq.py:253,261 (see ora_projection_rounding).
 #ifndef ORA_WORLD_FUSED_ABOVE
-#define ORA_WORLD_FUSED_ABOVE 1000
+#define ORA_WORLD_FUSED_ABOVE 1536
 #endif
 #ifndef ORA_IMAGE_FUSED_ABOVE
-#define ORA_IMAGE_FUSED_ABOVE 100000
+#define ORA_IMAGE_FUSED_ABOVE 233023
 #endif
 
 namespace {

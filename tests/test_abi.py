@@ -43,8 +43,16 @@ def test_version(L):
 def test_projection_rounding_matches_oracle(L):
     import oracle
     oracle.build()
-    for n in [0, 1, 999, 1000, 1001, 4099, 65536, 99999, 100000, 100001, 1_000_000, 3_000_000]:
+    for n in [0, 1, 2, 1536, 1537, 4099, 65536, 100000, 233023, 233024, 1_000_000, 3_000_000]:
         assert native.projection_rounding(n) == oracle.projection_rounding(n), n
+
+
+def test_projection_rounding_switch_points(L):
+    # measured on B200: cuBLAS fuses the w2c product from N=1537 and the K product from N=233024
+    assert native.projection_rounding(1536) == (0, 0)
+    assert native.projection_rounding(1537) == (1, 0)
+    assert native.projection_rounding(233023) == (1, 0)
+    assert native.projection_rounding(233024) == (1, 1)
 
 
 def test_workspace_size(L):

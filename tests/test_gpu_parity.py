@@ -165,8 +165,8 @@ def test_vs_oracle(case):
 def test_edge_cases():
     rng = np.random.default_rng(9)
     opt = synth.Options(kernel_size=3, radius_threshold=0.05, num_sample_points_per_ray=4, num_point_cloud_per_sp=8)
-    # every point projects to the same pixel: one bucket of 6000 (deep, sorted in global memory)
-    cam = synth.look_at_camera((0, 0, 4), (0, 0, 0), 16, 12, 0.5)
+    # every point projects to the same pixel (8, 6): one bucket of 6000 (deep, sorted in global memory)
+    cam = synth.look_at_camera((0, 0, 4), (0, 0, 0), 16, 12, 0.5, 0.5, 8.5, 6.5)
     xyz = (rng.normal(size=(6000, 3)) * 0.2).astype(np.float32)
     for sort in (False, True):
         (sidx, sdep, hsh), outs, dirs = _run_case(xyz, cam, opt, sort)
@@ -176,8 +176,8 @@ def test_edge_cases():
     # empty cloud
     (sidx, sdep, hsh), (sp_xyz, pc_idx, sp_t, mask), _ = _run_case(np.zeros((0, 3), np.float32), cam, opt, False)
     assert sidx.size == 0 and np.all(hsh == -1) and not mask.any() and np.all(pc_idx == -1) and np.all(sp_t == 0)
-    # all points off-image (behind/beside the camera): -1 everywhere
-    far = np.full((500, 3), 100.0, np.float32)
+    # all points off-image (beside the camera's field of view): -1 everywhere
+    far = np.tile(np.array([[100.0, 0.0, 0.0]], np.float32), (500, 1))
     (sidx, sdep, hsh), (sp_xyz, pc_idx, sp_t, mask), _ = _run_case(far, cam, opt, False)
     assert np.all(sidx == -1) and np.all(sdep == -1) and np.all(hsh == -1) and not mask.any()
     # 1x1, 1xW and Hx1 images
