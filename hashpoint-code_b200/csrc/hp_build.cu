@@ -24,6 +24,7 @@
 // point clouds (a few to a few hundred points per pixel) is far cheaper than
 // a serial sort per bucket, and every thread does useful work.
 #include <cstdio>
+#include <mutex>
 
 #include "hp_common.cuh"
 
@@ -333,7 +334,7 @@ __global__ void __launch_bounds__(256) k_runs(const int* __restrict__ point_idx,
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+static constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct BuildLayout {
   size_t counts, block_sums, pid_slot, depth, tmp_id, tmp_depth, tmp_pid, scalars, total;
@@ -484,4 +485,55 @@ extern "C" int32_t hp_scatter_hashtable(const int32_t* point_idx, const int32_t*
   // depth order inside each run, ties kept in input order
   return launch_order(hw, (int)n, (int)n, point_idx, depth, point2img, hash, nullptr, sorted_point_idx, sorted_depth,
                       BucketOrder{1, 1}, st);
+}
+
+// ---------------------------------------------------------------------------
+// hp_pts2plane_noalloc: hp_pts2plane over a scratch array built into the library
+// ---------------------------------------------------------------------------
+// For callers that cannot allocate device memory (see the header): the
+// scratch hp_pts2plane needs lives in this file-scope __device__ array, which
+// every GPU that loads the library holds until the process exits.  Sized for
+// the largest problem the entry point accepts.
+namespace hp {
+constexpr int64_t kNoAllocMaxPoints = HP_NOALLOC_MAX_POINTS;
+constexpr int64_t kNoAllocMaxPixels = HP_NOALLOC_MAX_PIXELS;
+constexpr size_t kNoAllocScratchBytes =
+    align256(sizeof(int) * kNoAllocMaxPixels) +
+    align256(sizeof(int) * ((kNoAllocMaxPixels + kScanTile - 1) / kScanTile)) +
+    align256(sizeof(int2) * kNoAllocMaxPoints) + 4 * align256(sizeof(float) * kNoAllocMaxPoints) + 256;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// (with that device current) on its first hp_pts2plane_noalloc call.
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[128] = {nullptr};
+}  // namespace hp
+
+extern "C" int32_t hp_pts2plane_noalloc(const float* xyz, int64_t n_points, const hp_camera* cam, int32_t sort,
+                                        int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table,
+                                        hp_stream_t stream) {
+  if (!cam) return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane_noalloc: cam is NULL");
+  const int64_t hw = (int64_t)cam->height * cam->width;
+  if (n_points > kNoAllocMaxPoints || hw > kNoAllocMaxPixels)
+    return set_error(HP_ERR_INVALID_ARGUMENT,
+                     "hp_pts2plane_noalloc: %lld points / %lld pixels exceed its built-in scratch "
+                     "(at most %lld points and %lld pixels); use hp_pts2plane with a workspace",
+                     (long long)n_points, (long long)hw, (long long)kNoAllocMaxPoints, (long long)kNoAllocMaxPixels);
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
+    return set_error(HP_ERR_CUDA, "hp_pts2plane_noalloc: cudaGetDevice failed (device %d)", dev);
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      const cudaError_t e = cudaGetSymbolAddress(&g_noalloc_addr[dev], g_noalloc_scratch);
+      if (e != cudaSuccess) {
+        g_noalloc_addr[dev] = nullptr;
+        return set_error(HP_ERR_CUDA, "hp_pts2plane_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+      }
+    }
+    scratch = g_noalloc_addr[dev];
+  }
+  return hp_pts2plane(xyz, n_points, cam, sort, sorted_point_idx, sorted_depth, hash_table, scratch,
+                      kNoAllocScratchBytes, stream);
 }

@@ -97,6 +97,26 @@ HP_API int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_camera*
                      int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table,
                      void* workspace, size_t workspace_bytes, hp_stream_t stream);
 
+/* hp_pts2plane for callers that cannot allocate device memory: a host plugin
+ * that only receives device pointers for its inputs and outputs from the
+ * application embedding it, or a service that must not grow its device
+ * footprint after start-up, has no way to provide hp_pts2plane's workspace.
+ * This entry point takes the same inputs and outputs and allocates nothing;
+ * its scratch is an array built into the library (about 10 MB of device
+ * memory on every GPU that loads the library, held until the process exits),
+ * so it accepts at most HP_NOALLOC_MAX_POINTS points and HP_NOALLOC_MAX_PIXELS
+ * pixels and returns HP_ERR_INVALID_ARGUMENT beyond that.  The first call on a
+ * device looks up that device's address of the array (make it before any
+ * stream capture).  All calls share the one array, so calls that overlap on
+ * the GPU (on different streams, or from different threads) race: serialise
+ * them.  Each call clears the parts of the array that must start at zero.
+ * No counterpart in the reference. */
+#define HP_NOALLOC_MAX_POINTS 262144
+#define HP_NOALLOC_MAX_PIXELS 1048576
+HP_API int32_t hp_pts2plane_noalloc(const float* xyz, int64_t n_points, const hp_camera* cam, int32_t sort,
+                                    int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table,
+                                    hp_stream_t stream);
+
 /* Per-pixel hash table from inputs already sorted by pixel id.  Replaces
  * _C.scatter_hashtable (epcq/csrc/rasterization.cu:130-171, kernel :7-34):
  * point_idx / point2img / depth [n] sorted by point2img ascending; entries with
