@@ -6,7 +6,7 @@
 // per ray, one lane per window cell, a 128-bin shared-memory histogram built
 // with float atomics and a serial walk on lane 0) and then
 // quick_search_nearby_pc (:10-81, one thread per (ray, sample slot) re-walking
-// the window).  Here a CTA owns a 4x32 pixel tile: it stages the points of
+// the window).  Here a CTA owns an 8x32 pixel tile: it stages the points of
 // the tile's window halo (clamped to the image) into shared memory once as
 // float4 (x, y, z, id) with coalesced gathers, then one thread owns one ray
 // end to end and writes every output element of that ray exactly once:
@@ -29,9 +29,13 @@
 //           skipped before the distance is computed: they cannot be within
 //           the radius, so the buffer sees exactly the same sequence.
 //
-// Each pass walks the ray's window as one flat candidate sequence, so the
-// lanes of a warp (32 neighbouring pixels, whose windows overlap) run loops of
-// similar length instead of diverging on every cell's bucket size.  Tiles
+// Each pass walks the ray's window as one flat candidate sequence, and the
+// tile's rays are ranked by window size before they are handed to threads, so
+// the lanes of a warp run loops of similar length instead of diverging on
+// every cell's bucket size.  The radius test decides on the squared distance
+// when it is clear of the threshold and calls norm3df only near it (see
+// RadiusTest); the mean distance of a bin is computed only for bins the walk
+// can reach.  Tiles
 // whose halo holds more than kStageCap points read candidates straight from
 // global memory through the same code.
 //
@@ -39,16 +43,18 @@
 // adds them with shared-memory atomics in an unspecified order, so a bin's
 // mean distance can differ from the reference's in the last bit -- which moves
 // an output only if alpha * T or T sits within that bit of 1e-3.
+#include <mutex>
+
 #include "hp_common.cuh"
 
 namespace hp {
 
 constexpr int kTileW = 32;   // pixels of one image row per warp
-constexpr int kTileH = 4;    // rows per block
+constexpr int kTileH = 8;    // rows per block
 constexpr int kThreads = kTileW * kTileH;
 constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
 constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
-constexpr int kStageCap = 2048;  // staged points per tile (32 KB)
+constexpr int kStageCap = 3072;  // staged points per tile (48 KB)
 constexpr int kBinList = 4;      // distinct t-bins collected per candidate pass
 constexpr int kTeReg = 4;        // emitted sample depths kept in registers
 
@@ -68,6 +74,8 @@ struct SampleArgs {
 
 struct Stage {
   float4 cand[kStageCap];  // x, y, z, id (as int bits; -1 = invalid id)
+  int4 work[kThreads / 4]; // per pixel of the tile: (window candidates << 8) | pixel
+  int order[kThreads];     // pixel each thread processes, most work first
   int off[kHaloMax + 1];   // staged offset of each halo cell, exclusive prefix
   int start[kHaloMax];     // the cell's first index in sorted_point_idx
   int warp_tot[kThreads / 32];
@@ -140,6 +148,45 @@ __device__ __forceinline__ void fill_run(T* p, int n, T v) {
   for (; i < n; i++) p[i] = v;
 }
 
+// The reference keeps a candidate when norm3df(e) < radius (e = point minus its
+// projection on the ray).  The squared length e2 (three roundings) decides it
+// without the square root whenever e2 is outside a band of relative width
+// 2^-16 around radius^2 -- far wider than the few-ulp errors of e2 and
+// norm3df -- and norm3df decides inside the band, so the result is identical.
+struct RadiusTest {
+  float r, lo2, hi2;
+  bool fast;
+};
+
+__device__ __forceinline__ RadiusTest make_radius_test(float r) {
+  RadiusTest rt;
+  rt.r = r;
+  const double r2 = (double)r * (double)r;
+  rt.fast = r2 > 1e-30 && r2 < 1e30;
+  rt.lo2 = (float)(r2 * (1.0 - 1.0 / 65536.0));
+  rt.hi2 = (float)(r2 * (1.0 + 1.0 / 65536.0));
+  return rt;
+}
+
+__device__ __forceinline__ bool within_radius(const RadiusTest& rt, float e0, float e1, float e2) {
+  if (rt.fast) {
+    const float q = __fmaf_rn(e2, e2, __fmaf_rn(e1, e1, __fmul_rn(e0, e0)));
+    if (q < rt.lo2) return true;
+    if (q > rt.hi2) return false;
+  }
+  return norm3df(e0, e1, e2) < rt.r;
+}
+
+// PointRayInterset's t (cuda_util.cuh:227); dividing by d.d == 1 is exact, so it is skipped then.
+__device__ __forceinline__ float ray_t(const Ray& r, bool unit, float px, float py, float pz, float& s0, float& s1,
+                                      float& s2) {
+  s0 = __fsub_rn(px, r.o[0]);
+  s1 = __fsub_rn(py, r.o[1]);
+  s2 = __fsub_rn(pz, r.o[2]);
+  const float num = dot3(s0, s1, s2, r.d[0], r.d[1], r.d[2]);
+  return unit ? num : __fdiv_rn(num, r.dd);
+}
+
 template <class Src>
 __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, int v, int u) {
   const int W = a.cam.width;
@@ -150,6 +197,8 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
 
   Ray r;
   make_ray(a.cam.c2w, a.cam.fx, a.cam.fy, a.cam.cx, a.cam.cy, u, v, r);
+  const bool unit = r.dd == 1.0f;
+  const RadiusTest rt = make_radius_test(radius);
 
   // pass A: tmin / tmax over the kept candidates (epcq_render_topk.cu:132-161)
   float tmin = 1e3f, tmax = -1e3f;
@@ -158,9 +207,12 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
     while (walk_next(w, src, a, v, u, ncell, kKeptPerCell)) {
       const float4 p = src.fetch(a, w.j++);
       if (__float_as_int(p.w) < 0) continue;
-      float t, dist;
-      intersect(r, p.x, p.y, p.z, t, dist);
-      if (dist < radius) {
+      float s0, s1, s2;
+      const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
+      const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
+      const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
+      const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
+      if (within_radius(rt, e0, e1, e2)) {
         w.nk++;
         if (tmin > t) tmin = t;
         if (tmax < t) tmax = t;
@@ -191,12 +243,20 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
       while (walk_next(w, src, a, v, u, ncell, kKeptPerCell)) {
         const float4 p = src.fetch(a, w.j++);
         if (__float_as_int(p.w) < 0) continue;
-        float t, dist;
-        intersect(r, p.x, p.y, p.z, t, dist);
-        if (!(dist < radius)) continue;
+        float s0, s1, s2;
+        const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
+        const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
+        const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
+        const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
+        if (!within_radius(rt, e0, e1, e2)) continue;
         w.nk++;
         const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
         if (b < lo || b >= cut) continue;
+        if (m == kBinList && b > lb[kBinList - 1]) {
+          cut = b;
+          continue;
+        }
+        const float dist = norm3df(e0, e1, e2);
         bool found = false;
 #pragma unroll
         for (int q = 0; q < kBinList; q++)
@@ -206,10 +266,6 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
             found = true;
           }
         if (found) continue;
-        if (m == kBinList && b > lb[kBinList - 1]) {
-          cut = b;
-          continue;
-        }
         int pos = 0;
 #pragma unroll
         for (int q = 0; q < kBinList; q++) pos += (q < m && lb[q] < b) ? 1 : 0;
@@ -395,7 +451,38 @@ __global__ void __launch_bounds__(kThreads) k_quick_sampling(SampleArgs a) {
     __syncthreads();
   }
 
-  const int u = u0 + lane, v = v0 + warp;
+  // Rank the tile's rays by their window's candidate count so each warp gets
+  // rays of similar work (the flat loops then diverge little).
+  {
+    const int pu = u0 + (tid & 31), pv = v0 + (tid >> 5);
+    int work = 0;
+    if (pu < W && pv < H) {
+      work = 1;
+      if (staged) {
+        const SrcStaged ss{&st, rv0, ru0, nu};
+        for (int l = 0; l < k * k; l++) {
+          int vv, uu;
+          window_cell(pv, pu, k, H, W, l, vv, uu);
+          const int2 rg = ss.range(a, vv, uu);
+          work += rg.y - rg.x;
+        }
+      }
+    }
+    int* work_flat = reinterpret_cast<int*>(st.work);
+    work_flat[tid] = (min(work, 0x7fffff) << 8) | tid;
+    __syncthreads();
+    const int mine = work_flat[tid];
+    int rank = 0;
+#pragma unroll 8
+    for (int q = 0; q < kThreads / 4; q++) {
+      const int4 w4 = st.work[q];
+      rank += (w4.x > mine) + (w4.y > mine) + (w4.z > mine) + (w4.w > mine);
+    }
+    st.order[rank] = tid;
+    __syncthreads();
+  }
+  const int px = st.order[tid];
+  const int u = u0 + (px & 31), v = v0 + (px >> 5);
   if (u >= W || v >= H) return;
   if (staged)
     sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v, u);
@@ -411,6 +498,24 @@ __global__ void k_ray_directions(DevCamera cam, float* __restrict__ dirs) {
   dirs[3 * (size_t)p + 0] = r.d[0];
   dirs[3 * (size_t)p + 1] = r.d[1];
   dirs[3 * (size_t)p + 2] = r.d[2];
+}
+
+// The stage exceeds the 48 KB default of dynamic shared memory: opt the kernel
+// in once per device.
+int32_t allow_stage_smem() {
+  static std::mutex mu;
+  static bool done[128] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
+    return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaGetDevice failed");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!done[dev]) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_quick_sampling, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Stage));
+    if (e != cudaSuccess) return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaFuncSetAttribute: %s", cudaGetErrorString(e));
+    done[dev] = true;
+  }
+  return HP_OK;
 }
 
 int32_t check_camera(const hp_camera* cam, const char* who) {
@@ -488,6 +593,7 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   a.sp_t = sp_t;
   a.mask = mask;
   const dim3 grid((cam->width + kTileW - 1) / kTileW, (cam->height + kTileH - 1) / kTileH);
+  if (int32_t rc = allow_stage_smem()) return rc;
   k_quick_sampling<<<grid, kThreads, sizeof(Stage), (cudaStream_t)stream>>>(a);
   return check_launch("k_quick_sampling");
 }
