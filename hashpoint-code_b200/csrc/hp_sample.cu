@@ -89,10 +89,12 @@ __device__ __forceinline__ int2 bucket_range(int2 h, int n_sorted) {
 
 // Candidates from the tile's shared-memory stage.
 struct SrcStaged {
+  static constexpr bool kStaged = true;
   const Stage* st;
   int rv0, ru0, nu;
+  __device__ __forceinline__ int cell(int vv, int uu) const { return (vv - rv0) * nu + (uu - ru0); }
   __device__ __forceinline__ int2 range(const SampleArgs&, int vv, int uu) const {
-    const int c = (vv - rv0) * nu + (uu - ru0);
+    const int c = cell(vv, uu);
     return make_int2(st->off[c], st->off[c + 1]);
   }
   __device__ __forceinline__ float4 fetch(const SampleArgs&, int i) const { return st->cand[i]; }
@@ -100,6 +102,8 @@ struct SrcStaged {
 
 // Candidates straight from global memory (tiles whose halo overflows the stage).
 struct SrcGlobal {
+  static constexpr bool kStaged = false;
+  __device__ __forceinline__ int cell(int, int) const { return 0; }
   __device__ __forceinline__ int2 range(const SampleArgs& a, int vv, int uu) const {
     return bucket_range(__ldg(a.hash + (size_t)vv * a.cam.width + uu), a.n_sorted);
   }
@@ -111,25 +115,57 @@ struct SrcGlobal {
   }
 };
 
-// A flat walk over the candidates of window cells 0..ncell-1 (row-major,
-// clamped), at most `cap` accepted per cell (the caller counts acceptances in nk).
-struct Walk {
-  int l, j, end, nk;
-};
-
-template <class Src>
-__device__ __forceinline__ bool walk_next(Walk& w, const Src& src, const SampleArgs& a, int v, int u, int ncell,
-                                          int cap) {
-  while (w.j >= w.end || w.nk >= cap) {
-    if (++w.l >= ncell) return false;
-    int vv, uu;
-    window_cell(v, u, a.opt.k, a.cam.height, a.cam.width, w.l, vv, uu);
-    const int2 r = src.range(a, vv, uu);
-    w.j = r.x;
-    w.end = r.y;
-    w.nk = 0;
+// Visit a ray's window candidates in the reference's order -- window rows
+// top to bottom, cells left to right (coordinates clamped into the image, so
+// border windows repeat cells), entries in bucket order -- calling
+// body(point) for each; body returns true when it accepts the candidate, and
+// a cell is left once `cap` of its candidates were accepted.
+//
+// Staged tiles: a window row whose columns need no clamping is a run of
+// consecutive halo cells, i.e. one contiguous range of the stage, so the loop
+// only watches for cell boundaries (for the cap).  Other rows, and tiles read
+// from global memory, go cell by cell.  No integer division per cell.
+template <class Src, class Body>
+__device__ __forceinline__ void walk_window(const SampleArgs& a, const Src& src, int v, int u, int cap, Body&& body) {
+  const int H = a.cam.height, W = a.cam.width, k = a.opt.k;
+  const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
+  const bool cols_clamped = (u - lo < 0) || (u + hi > W - 1);
+  for (int dv = -lo; dv <= hi; dv++) {
+    const int vv = min(max(v + dv, 0), H - 1);
+    bool done_row = false;
+    if constexpr (Src::kStaged) {
+      if (!cols_clamped) {
+        const int c0 = src.cell(vv, u - lo);
+        const int* off = src.st->off;
+        int j = off[c0];
+        const int jend = off[c0 + k];
+        int c = c0, cell_end = off[c0 + 1], nk = 0;
+        while (j < jend) {
+          while (j >= cell_end) {  // entered the next non-empty cell
+            c++;
+            cell_end = off[c + 1];
+            nk = 0;
+          }
+          if (nk >= cap) {
+            j = cell_end;
+            continue;
+          }
+          if (body(src.fetch(a, j))) nk++;
+          j++;
+        }
+        done_row = true;
+      }
+    }
+    if (!done_row) {
+      for (int du = -lo; du <= hi; du++) {
+        const int uu = min(max(u + du, 0), W - 1);
+        const int2 rg = src.range(a, vv, uu);
+        int nk = 0;
+        for (int j = rg.x; j < rg.y && nk < cap; j++)
+          if (body(src.fetch(a, j))) nk++;
+      }
+    }
   }
-  return true;
 }
 
 // Fill n elements from p with v using 16-byte stores where aligned.
@@ -191,8 +227,7 @@ template <class Src>
 __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, int v, int u) {
   const int W = a.cam.width;
   const int ray = v * W + u;
-  const int S = a.opt.S, P = a.opt.P, k = a.opt.k, k2 = k * k;
-  const int ncell = k2 < kLaneCells ? k2 : kLaneCells;
+  const int S = a.opt.S, P = a.opt.P;
   const float radius = a.opt.radius;
 
   Ray r;
@@ -202,23 +237,18 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
 
   // pass A: tmin / tmax over the kept candidates (epcq_render_topk.cu:132-161)
   float tmin = 1e3f, tmax = -1e3f;
-  {
-    Walk w{-1, 0, 0, 0};
-    while (walk_next(w, src, a, v, u, ncell, kKeptPerCell)) {
-      const float4 p = src.fetch(a, w.j++);
-      if (__float_as_int(p.w) < 0) continue;
-      float s0, s1, s2;
-      const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
-      const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
-      const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
-      const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
-      if (within_radius(rt, e0, e1, e2)) {
-        w.nk++;
-        if (tmin > t) tmin = t;
-        if (tmax < t) tmax = t;
-      }
-    }
-  }
+  walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
+    if (__float_as_int(p.w) < 0) return false;
+    float s0, s1, s2;
+    const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
+    const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
+    const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
+    const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
+    if (!within_radius(rt, e0, e1, e2)) return false;
+    if (tmin > t) tmin = t;
+    if (tmax < t) tmax = t;
+    return true;
+  });
 
   float* o_xyz = a.sp_xyz + (size_t)ray * S * 3;
   float* o_t = a.sp_t + (size_t)ray * S;
@@ -239,22 +269,19 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
 #pragma unroll
       for (int q = 0; q < kBinList; q++) lb[q] = 0x7fffffff, lc[q] = 0, ls[q] = 0.0f;
       int m = 0, cut = kBins;
-      Walk w{-1, 0, 0, 0};
-      while (walk_next(w, src, a, v, u, ncell, kKeptPerCell)) {
-        const float4 p = src.fetch(a, w.j++);
-        if (__float_as_int(p.w) < 0) continue;
+      walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
+        if (__float_as_int(p.w) < 0) return false;
         float s0, s1, s2;
         const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
         const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
         const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
         const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
-        if (!within_radius(rt, e0, e1, e2)) continue;
-        w.nk++;
+        if (!within_radius(rt, e0, e1, e2)) return false;
         const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
-        if (b < lo || b >= cut) continue;
+        if (b < lo || b >= cut) return true;
         if (m == kBinList && b > lb[kBinList - 1]) {
           cut = b;
-          continue;
+          return true;
         }
         const float dist = norm3df(e0, e1, e2);
         bool found = false;
@@ -265,7 +292,7 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
             ls[q] = __fadd_rn(ls[q], dist);
             found = true;
           }
-        if (found) continue;
+        if (found) return true;
         int pos = 0;
 #pragma unroll
         for (int q = 0; q < kBinList; q++) pos += (q < m && lb[q] < b) ? 1 : 0;
@@ -283,7 +310,8 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
           }
         }
         m = m < kBinList ? m + 1 : kBinList;
-      }
+        return true;
+      });
       // primary-surface walk (epcq_render_topk.cu:181-204)
       bool done = false;
 #pragma unroll
@@ -333,15 +361,13 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
     for (int q = 0; q < kBallBuf; q++) bd[q] = 0.0f, bi[q] = -1;
     int bsize = 0, maxi = 0;
     float maxd = 1e3f;
-    Walk w{-1, 0, 0, 0};
-    while (walk_next(w, src, a, v, u, k2, 0x7fffffff)) {
-      const float4 p = src.fetch(a, w.j++);
+    walk_window(a, src, v, u, 0x7fffffff, [&](const float4& p) -> bool {
       const int id = __float_as_int(p.w);
-      if (id < 0) continue;
+      if (id < 0) return false;
       const float along = dot3(p.x - r.o[0], p.y - r.o[1], p.z - r.o[2], r.d[0], r.d[1], r.d[2]);
-      if (fabsf(along - ts) > reach) continue;
+      if (fabsf(along - ts) > reach) return false;
       const float dist = norm3df(__fsub_rn(sx, p.x), __fsub_rn(sy, p.y), __fsub_rn(sz, p.z));
-      if (!(dist < radius)) continue;
+      if (!(dist < radius)) return false;
       if (bsize < kBallBuf) {
 #pragma unroll
         for (int q = 0; q < kBallBuf; q++)
@@ -363,7 +389,8 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
             maxi = q;
           }
       }
-    }
+      return false;
+    });
     int* row = o_idx + (size_t)s * P;
 #pragma unroll
     for (int q = 0; q < kBallBuf; q++)
@@ -380,7 +407,7 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_quick_sampling(SampleArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Stage& st = *reinterpret_cast<Stage*>(smem_raw);
   const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
