@@ -8,8 +8,9 @@
 // quick_search_nearby_pc (:10-81, one thread per (ray, sample slot) re-walking
 // the window).  Here a CTA owns an 8x32 pixel tile: it stages the points of
 // the tile's window halo (clamped to the image) into shared memory once as
-// float4 (x, y, z, id) with coalesced gathers, then one thread owns one ray
-// end to end and writes every output element of that ray exactly once:
+// float4 (x, y, z, id) with coalesced gathers (bands of rows when the whole
+// halo does not fit), then one thread owns one ray end to end and writes
+// every output element of that ray exactly once:
 //
 //   pass A  kept candidates (ray distance < radius, at most 48 per window cell,
 //           cells row-major and clamped, bucket order) -> tmin, tmax
@@ -35,9 +36,9 @@
 // every cell's bucket size.  The radius test decides on the squared distance
 // when it is clear of the threshold and calls norm3df only near it (see
 // RadiusTest); the mean distance of a bin is computed only for bins the walk
-// can reach.  Tiles
-// whose halo holds more than kStageCap points read candidates straight from
-// global memory through the same code.
+// can reach.  A one-row band whose halo still holds more than kStageCap
+// points reads its candidates straight from global memory through the same
+// code.
 //
 // Bin sums are accumulated in window-cell then bucket order; the reference
 // adds them with shared-memory atomics in an unspecified order, so a bin's
@@ -54,7 +55,7 @@ constexpr int kTileH = 8;    // rows per block
 constexpr int kThreads = kTileW * kTileH;
 constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
 constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
-constexpr int kStageCap = 3072;  // staged points per tile (48 KB)
+constexpr int kStageCap = 4096;  // staged points per band (64 KB)
 constexpr int kBinList = 4;      // distinct t-bins collected per candidate pass
 constexpr int kTeReg = 4;        // emitted sample depths kept in registers
 
@@ -100,7 +101,7 @@ struct SrcStaged {
   __device__ __forceinline__ float4 fetch(const SampleArgs&, int i) const { return st->cand[i]; }
 };
 
-// Candidates straight from global memory (tiles whose halo overflows the stage).
+// Candidates straight from global memory (one-row bands whose halo overflows the stage).
 struct SrcGlobal {
   static constexpr bool kStaged = false;
   __device__ __forceinline__ int cell(int, int) const { return 0; }
@@ -407,26 +408,31 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Stage& st = *reinterpret_cast<Stage*>(smem_raw);
+// Cell table of the halo of rows [vb, vb + rows) of the tile's columns: global
+// start and clipped count per halo cell, block-wide exclusive prefix in
+// st.off.  Returns the number of points in the halo (every thread gets it).
+struct Band {
+  int vb, rows, rv0, ru0, nu, ncells;
+};
+
+__device__ __forceinline__ int stage_table(const SampleArgs& a, Stage& st, Band& bd, int u0) {
   const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
   const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
-  const int v0 = blockIdx.y * kTileH, u0 = blockIdx.x * kTileW;
-  const int rv0 = max(0, v0 - lo), rv1 = min(H - 1, v0 + kTileH - 1 + hi);
-  const int ru0 = max(0, u0 - lo), ru1 = min(W - 1, u0 + kTileW - 1 + hi);
-  const int nu = ru1 - ru0 + 1, ncells = (rv1 - rv0 + 1) * nu;
+  bd.rv0 = max(0, bd.vb - lo);
+  const int rv1 = min(H - 1, bd.vb + bd.rows - 1 + hi);
+  bd.ru0 = max(0, u0 - lo);
+  const int ru1 = min(W - 1, u0 + kTileW - 1 + hi);
+  bd.nu = ru1 - bd.ru0 + 1;
+  bd.ncells = (rv1 - bd.rv0 + 1) * bd.nu;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-
-  // halo cell table: global start, clipped count, block-wide exclusive prefix
   int cnt[kCellsPerThread];
   int local = 0;
 #pragma unroll
   for (int q = 0; q < kCellsPerThread; q++) {
     const int c = tid * kCellsPerThread + q;
     cnt[q] = 0;
-    if (c < ncells) {
-      const int vv = rv0 + c / nu, uu = ru0 + c % nu;
+    if (c < bd.ncells) {
+      const int vv = bd.rv0 + c / bd.nu, uu = bd.ru0 + c % bd.nu;
       const int2 rg = bucket_range(__ldg(a.hash + (size_t)vv * W + uu), a.n_sorted);
       st.start[c] = rg.x;
       // capped so the prefix cannot overflow; a capped cell alone exceeds the stage
@@ -440,6 +446,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a) {
     const int t = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += t;
   }
+  __syncthreads();  // previous readers of st are done
   if (lane == 31) st.warp_tot[warp] = incl;
   __syncthreads();
   int base = incl - local;
@@ -450,71 +457,97 @@ __global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a) {
 #pragma unroll
   for (int q = 0; q < kCellsPerThread; q++) {
     const int c = tid * kCellsPerThread + q;
-    if (c < ncells) st.off[c] = base;
+    if (c < bd.ncells) st.off[c] = base;
     base += cnt[q];
   }
-  if (tid == 0) st.off[ncells] = total;
+  if (tid == 0) st.off[bd.ncells] = total;
   __syncthreads();
+  return total;
+}
 
-  const bool staged = total <= kStageCap;
-  if (staged) {
-    for (int i = tid; i < total; i += kThreads) {
-      int lo_c = 0, hi_c = ncells;  // off[lo_c] <= i < off[hi_c]
-      while (hi_c - lo_c > 1) {
-        const int mid = (lo_c + hi_c) >> 1;
-        if (st.off[mid] <= i)
-          lo_c = mid;
-        else
-          hi_c = mid;
-      }
-      const int id = __ldg(a.sidx + st.start[lo_c] + (i - st.off[lo_c]));
-      float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-      if ((unsigned)id < (unsigned)a.n_points) {
-        const float4 q = load_point(a.xyz, id);
-        p = make_float4(q.x, q.y, q.z, __int_as_float(id));
-      }
-      st.cand[i] = p;
+__device__ __forceinline__ void stage_points(const SampleArgs& a, Stage& st, const Band& bd, int total) {
+  for (int i = threadIdx.x; i < total; i += kThreads) {
+    int lo_c = 0, hi_c = bd.ncells;  // off[lo_c] <= i < off[hi_c]
+    while (hi_c - lo_c > 1) {
+      const int mid = (lo_c + hi_c) >> 1;
+      if (st.off[mid] <= i)
+        lo_c = mid;
+      else
+        hi_c = mid;
     }
-    __syncthreads();
+    const int id = __ldg(a.sidx + st.start[lo_c] + (i - st.off[lo_c]));
+    float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    if ((unsigned)id < (unsigned)a.n_points) {
+      const float4 q = load_point(a.xyz, id);
+      p = make_float4(q.x, q.y, q.z, __int_as_float(id));
+    }
+    st.cand[i] = p;
   }
+  __syncthreads();
+}
 
-  // Rank the tile's rays by their window's candidate count so each warp gets
-  // rays of similar work (the flat loops then diverge little).
-  {
-    const int pu = u0 + (tid & 31), pv = v0 + (tid >> 5);
-    int work = 0;
-    if (pu < W && pv < H) {
-      work = 1;
-      if (staged) {
-        const SrcStaged ss{&st, rv0, ru0, nu};
-        for (int l = 0; l < k * k; l++) {
-          int vv, uu;
-          window_cell(pv, pu, k, H, W, l, vv, uu);
-          const int2 rg = ss.range(a, vv, uu);
-          work += rg.y - rg.x;
+// A CTA owns an 8x32 tile.  It stages the halo of the whole tile when it fits
+// in the stage, otherwise of bands of 4, 2 or 1 rows in turn (a one-row band
+// that still overflows reads global memory).  The band's rays are ranked by
+// window size and handed out most-work-first.
+__global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Stage& st = *reinterpret_cast<Stage*>(smem_raw);
+  const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
+  const int v0 = blockIdx.y * kTileH, u0 = blockIdx.x * kTileW;
+  const int v_end = min(H, v0 + kTileH);
+  const int tid = threadIdx.x;
+  for (int vb = v0; vb < v_end;) {
+    Band bd;
+    bd.vb = vb;
+    bd.rows = v_end - vb;
+    int total = stage_table(a, st, bd, u0);
+    while (total > kStageCap && bd.rows > 1) {
+      bd.rows = (bd.rows + 1) >> 1;
+      total = stage_table(a, st, bd, u0);
+    }
+    const bool staged = total <= kStageCap;
+    if (staged) stage_points(a, st, bd, total);
+    const int nrays = bd.rows * kTileW;
+    // rank the band's rays by window size (most work first)
+    {
+      const int pu = u0 + (tid & 31), pv = vb + (tid >> 5);
+      int work = 0;
+      if (tid < nrays && pu < W) {
+        work = 1;
+        if (staged) {
+          const SrcStaged ss{&st, bd.rv0, bd.ru0, bd.nu};
+          for (int l = 0; l < k * k; l++) {
+            int vv, uu;
+            window_cell(pv, pu, k, H, W, l, vv, uu);
+            const int2 rg = ss.range(a, vv, uu);
+            work += rg.y - rg.x;
+          }
         }
       }
-    }
-    int* work_flat = reinterpret_cast<int*>(st.work);
-    work_flat[tid] = (min(work, 0x7fffff) << 8) | tid;
-    __syncthreads();
-    const int mine = work_flat[tid];
-    int rank = 0;
+      int* work_flat = reinterpret_cast<int*>(st.work);
+      work_flat[tid] = (min(work, 0x7fffff) << 8) | tid;
+      __syncthreads();
+      const int mine = work_flat[tid];
+      int rank = 0;
 #pragma unroll 8
-    for (int q = 0; q < kThreads / 4; q++) {
-      const int4 w4 = st.work[q];
-      rank += (w4.x > mine) + (w4.y > mine) + (w4.z > mine) + (w4.w > mine);
+      for (int q = 0; q < kThreads / 4; q++) {
+        const int4 w4 = st.work[q];
+        rank += (w4.x > mine) + (w4.y > mine) + (w4.z > mine) + (w4.w > mine);
+      }
+      st.order[rank] = tid;
+      __syncthreads();
     }
-    st.order[rank] = tid;
-    __syncthreads();
+    const int px = st.order[tid];
+    const int u = u0 + (px & 31), v = vb + (px >> 5);
+    if (px < nrays && u < W) {
+      if (staged)
+        sample_ray(a, SrcStaged{&st, bd.rv0, bd.ru0, bd.nu}, v, u);
+      else
+        sample_ray(a, SrcGlobal{}, v, u);
+    }
+    vb += bd.rows;
   }
-  const int px = st.order[tid];
-  const int u = u0 + (px & 31), v = v0 + (px >> 5);
-  if (u >= W || v >= H) return;
-  if (staged)
-    sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v, u);
-  else
-    sample_ray(a, SrcGlobal{}, v, u);
 }
 
 __global__ void k_ray_directions(DevCamera cam, float* __restrict__ dirs) {
