@@ -8,9 +8,8 @@
 // quick_search_nearby_pc (:10-81, one thread per (ray, sample slot) re-walking
 // the window).  Here a CTA owns an 8x32 pixel tile: it stages the points of
 // the tile's window halo (clamped to the image) into shared memory once as
-// float4 (x, y, z, id) with coalesced gathers (bands of rows when the whole
-// halo does not fit), then one thread owns one ray end to end and writes
-// every output element of that ray exactly once:
+// float4 (x, y, z, id) with coalesced gathers, then one thread owns one ray
+// end to end and writes every output element of that ray exactly once:
 //
 //   pass A  kept candidates (ray distance < radius, at most 48 per window cell,
 //           cells row-major and clamped, bucket order) -> tmin, tmax
@@ -36,9 +35,9 @@
 // every cell's bucket size.  The radius test decides on the squared distance
 // when it is clear of the threshold and calls norm3df only near it (see
 // RadiusTest); the mean distance of a bin is computed only for bins the walk
-// can reach.  A one-row band whose halo still holds more than kStageCap
-// points reads its candidates straight from global memory through the same
-// code.
+// can reach.  Tiles
+// whose halo holds more than kStageCap points read candidates straight from
+// global memory through the same code.
 //
 // Bin sums are accumulated in window-cell then bucket order; the reference
 // adds them with shared-memory atomics in an unspecified order, so a bin's
@@ -55,7 +54,7 @@ constexpr int kTileH = 8;    // rows per block
 constexpr int kThreads = kTileW * kTileH;
 constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
 constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
-constexpr int kStageCap = 4096;  // staged points per band (64 KB)
+constexpr int kStageCap = 4096;  // staged points per tile (64 KB)
 constexpr int kBinList = 4;      // distinct t-bins collected per candidate pass
 constexpr int kTeReg = 4;        // emitted sample depths kept in registers
 
@@ -101,7 +100,7 @@ struct SrcStaged {
   __device__ __forceinline__ float4 fetch(const SampleArgs&, int i) const { return st->cand[i]; }
 };
 
-// Candidates straight from global memory (one-row bands whose halo overflows the stage).
+// Candidates straight from global memory (tiles whose halo overflows the stage).
 struct SrcGlobal {
   static constexpr bool kStaged = false;
   __device__ __forceinline__ int cell(int, int) const { return 0; }
@@ -408,31 +407,78 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
   }
 }
 
-// Cell table of the halo of rows [vb, vb + rows) of the tile's columns: global
-// start and clipped count per halo cell, block-wide exclusive prefix in
-// st.off.  Returns the number of points in the halo (every thread gets it).
-struct Band {
-  int vb, rows, rv0, ru0, nu, ncells;
+// Tile scheduling.  A tile's cost grows with the points in its window halo
+// and is very uneven (dense objects vs background), so tiles are handed out
+// heaviest first (a counting sort on log2 of the halo's point count, with
+// halos too large to stage weighted up), to a persistent grid of
+// SMs x resident blocks that takes the next tile from an atomic counter.  The
+// heavy tiles then start first and the light ones fill in around them,
+// instead of a few heavy tiles finishing alone at the end.
+struct Sched {
+  int* work;    // [ntiles] estimated cost
+  int* order;   // [ntiles] tile ids, heaviest first
+  int* counts;  // [32] tiles per cost class
+  int* fill;    // [32] placement cursors
+  int* next;    // [1] next position in `order` to hand out
 };
 
-__device__ __forceinline__ int stage_table(const SampleArgs& a, Stage& st, Band& bd, int u0) {
+__device__ __forceinline__ int cost_class(int w) { return 31 - __clz(w | 1); }
+
+__global__ void __launch_bounds__(256) k_tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k,
+                                                   int tiles_x, int ntiles, Sched sc) {
+  const int lane = threadIdx.x & 31;
+  const int t = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (t >= ntiles) return;
+  const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
+  const int v0 = (t / tiles_x) * kTileH, u0 = (t % tiles_x) * kTileW;
+  const int rv0 = max(0, v0 - lo), rv1 = min(H - 1, v0 + kTileH - 1 + hi);
+  const int ru0 = max(0, u0 - lo), ru1 = min(W - 1, u0 + kTileW - 1 + hi);
+  const int nu = ru1 - ru0 + 1, ncells = (rv1 - rv0 + 1) * nu;
+  int sum = 0;
+  for (int c = lane; c < ncells; c += 32) {
+    const int2 rg = bucket_range(__ldg(hash + (size_t)(rv0 + c / nu) * W + ru0 + c % nu), n_sorted);
+    sum += min(rg.y - rg.x, kStageCap + 1);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if (lane == 0) {
+    const int w = sum > kStageCap ? min(sum, 1 << 26) * 4 : sum;  // unstaged tiles read global memory
+    sc.work[t] = w;
+    atomicAdd(sc.counts + cost_class(w), 1);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_tile_order(int ntiles, Sched sc) {
+  __shared__ int base[32];
+  if (threadIdx.x < 32) {
+    int b = 0;  // tiles in heavier classes
+    for (int c = 31; c > (int)threadIdx.x; c--) b += sc.counts[c];
+    base[threadIdx.x] = b;
+  }
+  __syncthreads();
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    const int c = cost_class(sc.work[t]);
+    sc.order[base[c] + atomicAdd(sc.fill + c, 1)] = t;
+  }
+}
+
+__device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int v0, int u0) {
   const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
   const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
-  bd.rv0 = max(0, bd.vb - lo);
-  const int rv1 = min(H - 1, bd.vb + bd.rows - 1 + hi);
-  bd.ru0 = max(0, u0 - lo);
-  const int ru1 = min(W - 1, u0 + kTileW - 1 + hi);
-  bd.nu = ru1 - bd.ru0 + 1;
-  bd.ncells = (rv1 - bd.rv0 + 1) * bd.nu;
+  const int rv0 = max(0, v0 - lo), rv1 = min(H - 1, v0 + kTileH - 1 + hi);
+  const int ru0 = max(0, u0 - lo), ru1 = min(W - 1, u0 + kTileW - 1 + hi);
+  const int nu = ru1 - ru0 + 1, ncells = (rv1 - rv0 + 1) * nu;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  // halo cell table: global start, clipped count, block-wide exclusive prefix
   int cnt[kCellsPerThread];
   int local = 0;
 #pragma unroll
   for (int q = 0; q < kCellsPerThread; q++) {
     const int c = tid * kCellsPerThread + q;
     cnt[q] = 0;
-    if (c < bd.ncells) {
-      const int vv = bd.rv0 + c / bd.nu, uu = bd.ru0 + c % bd.nu;
+    if (c < ncells) {
+      const int vv = rv0 + c / nu, uu = ru0 + c % nu;
       const int2 rg = bucket_range(__ldg(a.hash + (size_t)vv * W + uu), a.n_sorted);
       st.start[c] = rg.x;
       // capped so the prefix cannot overflow; a capped cell alone exceeds the stage
@@ -446,7 +492,6 @@ __device__ __forceinline__ int stage_table(const SampleArgs& a, Stage& st, Band&
     const int t = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += t;
   }
-  __syncthreads();  // previous readers of st are done
   if (lane == 31) st.warp_tot[warp] = incl;
   __syncthreads();
   int base = incl - local;
@@ -457,96 +502,83 @@ __device__ __forceinline__ int stage_table(const SampleArgs& a, Stage& st, Band&
 #pragma unroll
   for (int q = 0; q < kCellsPerThread; q++) {
     const int c = tid * kCellsPerThread + q;
-    if (c < bd.ncells) st.off[c] = base;
+    if (c < ncells) st.off[c] = base;
     base += cnt[q];
   }
-  if (tid == 0) st.off[bd.ncells] = total;
+  if (tid == 0) st.off[ncells] = total;
   __syncthreads();
-  return total;
-}
 
-__device__ __forceinline__ void stage_points(const SampleArgs& a, Stage& st, const Band& bd, int total) {
-  for (int i = threadIdx.x; i < total; i += kThreads) {
-    int lo_c = 0, hi_c = bd.ncells;  // off[lo_c] <= i < off[hi_c]
-    while (hi_c - lo_c > 1) {
-      const int mid = (lo_c + hi_c) >> 1;
-      if (st.off[mid] <= i)
-        lo_c = mid;
-      else
-        hi_c = mid;
+  const bool staged = total <= kStageCap;
+  if (staged) {
+    for (int i = tid; i < total; i += kThreads) {
+      int lo_c = 0, hi_c = ncells;  // off[lo_c] <= i < off[hi_c]
+      while (hi_c - lo_c > 1) {
+        const int mid = (lo_c + hi_c) >> 1;
+        if (st.off[mid] <= i)
+          lo_c = mid;
+        else
+          hi_c = mid;
+      }
+      const int id = __ldg(a.sidx + st.start[lo_c] + (i - st.off[lo_c]));
+      float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+      if ((unsigned)id < (unsigned)a.n_points) {
+        const float4 q = load_point(a.xyz, id);
+        p = make_float4(q.x, q.y, q.z, __int_as_float(id));
+      }
+      st.cand[i] = p;
     }
-    const int id = __ldg(a.sidx + st.start[lo_c] + (i - st.off[lo_c]));
-    float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-    if ((unsigned)id < (unsigned)a.n_points) {
-      const float4 q = load_point(a.xyz, id);
-      p = make_float4(q.x, q.y, q.z, __int_as_float(id));
-    }
-    st.cand[i] = p;
+    __syncthreads();
   }
-  __syncthreads();
+
+  // Rank the tile's rays by their window's candidate count so each warp gets
+  // rays of similar work (the flat loops then diverge little).
+  {
+    const int pu = u0 + (tid & 31), pv = v0 + (tid >> 5);
+    int work = 0;
+    if (pu < W && pv < H) {
+      work = 1;
+      for (int l = 0; l < k * k; l++) {
+        int vv, uu;
+        window_cell(pv, pu, k, H, W, l, vv, uu);
+        const int2 rg = staged ? SrcStaged{&st, rv0, ru0, nu}.range(a, vv, uu) : SrcGlobal{}.range(a, vv, uu);
+        work += rg.y - rg.x;
+      }
+    }
+    int* work_flat = reinterpret_cast<int*>(st.work);
+    work_flat[tid] = (min(work, 0x7fffff) << 8) | tid;
+    __syncthreads();
+    const int mine = work_flat[tid];
+    int rank = 0;
+#pragma unroll 8
+    for (int q = 0; q < kThreads / 4; q++) {
+      const int4 w4 = st.work[q];
+      rank += (w4.x > mine) + (w4.y > mine) + (w4.z > mine) + (w4.w > mine);
+    }
+    st.order[rank] = tid;
+    __syncthreads();
+  }
+  const int px = st.order[tid];
+  const int u = u0 + (px & 31), v = v0 + (px >> 5);
+  if (u < W && v < H) {
+    if (staged)
+      sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v, u);
+    else
+      sample_ray(a, SrcGlobal{}, v, u);
+  }
+  __syncthreads();  // the stage is reused by the next tile
 }
 
-// A CTA owns an 8x32 tile.  It stages the halo of the whole tile when it fits
-// in the stage, otherwise of bands of 4, 2 or 1 rows in turn (a one-row band
-// that still overflows reads global memory).  The band's rays are ranked by
-// window size and handed out most-work-first.
-__global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a, Sched sc, int tiles_x, int ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Stage& st = *reinterpret_cast<Stage*>(smem_raw);
-  const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
-  const int v0 = blockIdx.y * kTileH, u0 = blockIdx.x * kTileW;
-  const int v_end = min(H, v0 + kTileH);
-  const int tid = threadIdx.x;
-  for (int vb = v0; vb < v_end;) {
-    Band bd;
-    bd.vb = vb;
-    bd.rows = v_end - vb;
-    int total = stage_table(a, st, bd, u0);
-    while (total > kStageCap && bd.rows > 1) {
-      bd.rows = (bd.rows + 1) >> 1;
-      total = stage_table(a, st, bd, u0);
-    }
-    const bool staged = total <= kStageCap;
-    if (staged) stage_points(a, st, bd, total);
-    const int nrays = bd.rows * kTileW;
-    // rank the band's rays by window size (most work first)
-    {
-      const int pu = u0 + (tid & 31), pv = vb + (tid >> 5);
-      int work = 0;
-      if (tid < nrays && pu < W) {
-        work = 1;
-        if (staged) {
-          const SrcStaged ss{&st, bd.rv0, bd.ru0, bd.nu};
-          for (int l = 0; l < k * k; l++) {
-            int vv, uu;
-            window_cell(pv, pu, k, H, W, l, vv, uu);
-            const int2 rg = ss.range(a, vv, uu);
-            work += rg.y - rg.x;
-          }
-        }
-      }
-      int* work_flat = reinterpret_cast<int*>(st.work);
-      work_flat[tid] = (min(work, 0x7fffff) << 8) | tid;
-      __syncthreads();
-      const int mine = work_flat[tid];
-      int rank = 0;
-#pragma unroll 8
-      for (int q = 0; q < kThreads / 4; q++) {
-        const int4 w4 = st.work[q];
-        rank += (w4.x > mine) + (w4.y > mine) + (w4.z > mine) + (w4.w > mine);
-      }
-      st.order[rank] = tid;
-      __syncthreads();
-    }
-    const int px = st.order[tid];
-    const int u = u0 + (px & 31), v = vb + (px >> 5);
-    if (px < nrays && u < W) {
-      if (staged)
-        sample_ray(a, SrcStaged{&st, bd.rv0, bd.ru0, bd.nu}, v, u);
-      else
-        sample_ray(a, SrcGlobal{}, v, u);
-    }
-    vb += bd.rows;
+  __shared__ int s_next;
+  for (;;) {
+    if (threadIdx.x == 0) s_next = atomicAdd(sc.next, 1);
+    __syncthreads();
+    const int i = s_next;
+    if (i >= ntiles) break;
+    const int t = sc.order[i];
+    process_tile(a, st, (t / tiles_x) * kTileH, (t % tiles_x) * kTileW);
   }
 }
 
@@ -561,21 +593,42 @@ __global__ void k_ray_directions(DevCamera cam, float* __restrict__ dirs) {
 }
 
 // The stage exceeds the 48 KB default of dynamic shared memory: opt the kernel
-// in once per device.
-int32_t allow_stage_smem() {
+// in once per device and size the persistent grid from its occupancy.
+int32_t sampling_grid(int* blocks) {
   static std::mutex mu;
-  static bool done[128] = {false};
+  static int grid[128] = {0};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
     return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaGetDevice failed");
   std::lock_guard<std::mutex> lock(mu);
-  if (!done[dev]) {
-    const cudaError_t e =
+  if (!grid[dev]) {
+    cudaError_t e =
         cudaFuncSetAttribute(k_quick_sampling, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Stage));
-    if (e != cudaSuccess) return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-    done[dev] = true;
+    int sms = 0, per_sm = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_quick_sampling, kThreads, sizeof(Stage));
+    if (e != cudaSuccess) return set_error(HP_ERR_CUDA, "hp_quick_sampling: kernel set-up: %s", cudaGetErrorString(e));
+    grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
   }
+  *blocks = grid[dev];
   return HP_OK;
+}
+
+static constexpr size_t align256s(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct SchedLayout {
+  size_t work, order, small, total;
+};
+
+static SchedLayout sched_layout(int64_t H, int64_t W) {
+  const int64_t ntiles = ((W + kTileW - 1) / kTileW) * ((H + kTileH - 1) / kTileH);
+  SchedLayout L;
+  L.work = 0;
+  L.order = align256s(sizeof(int) * (size_t)ntiles);
+  L.small = L.order + align256s(sizeof(int) * (size_t)ntiles);
+  L.total = L.small + 512;  // counts[32], fill[32], next
+  return L;
 }
 
 int32_t check_camera(const hp_camera* cam, const char* who) {
@@ -615,9 +668,15 @@ DevOptions dev_options(const hp_options* o) {
 
 using namespace hp;
 
+extern "C" size_t hp_quick_sampling_workspace_size(int32_t height, int32_t width) {
+  if (height <= 0 || width <= 0) return 0;
+  return sched_layout(height, width).total;
+}
+
 extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const hp_camera* cam, const hp_options* opt,
                                      const int32_t* sorted_point_idx, int64_t n_sorted, const int32_t* hash_table,
-                                     float* sp_xyz, int32_t* pc_idx, float* sp_t, uint8_t* mask, hp_stream_t stream) {
+                                     float* sp_xyz, int32_t* pc_idx, float* sp_t, uint8_t* mask, void* workspace,
+                                     size_t workspace_bytes, hp_stream_t stream) {
   if (int32_t rc = check_camera(cam, "hp_quick_sampling")) return rc;
   if (!opt) return set_error(HP_ERR_INVALID_ARGUMENT, "hp_quick_sampling: opt is NULL");
   if (opt->kernel_size < 1 || opt->kernel_size > kMaxKernel)
@@ -640,6 +699,10 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
     return set_error(HP_ERR_INVALID_ARGUMENT, "hp_quick_sampling: null pointer");
   if (((uintptr_t)hash_table & 7) != 0)
     return set_error(HP_ERR_INVALID_ARGUMENT, "hp_quick_sampling: hash_table must be 8-byte aligned");
+  const SchedLayout L = sched_layout(cam->height, cam->width);
+  if (!workspace || workspace_bytes < L.total || ((uintptr_t)workspace & 255) != 0)
+    return set_error(HP_ERR_WORKSPACE, "hp_quick_sampling: workspace needs %zu bytes, 256-byte aligned (got %zu)",
+                     L.total, workspace_bytes);
   SampleArgs a;
   a.xyz = xyz;
   a.sidx = sorted_point_idx;
@@ -652,9 +715,26 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   a.pc_idx = pc_idx;
   a.sp_t = sp_t;
   a.mask = mask;
-  const dim3 grid((cam->width + kTileW - 1) / kTileW, (cam->height + kTileH - 1) / kTileH);
-  if (int32_t rc = allow_stage_smem()) return rc;
-  k_quick_sampling<<<grid, kThreads, sizeof(Stage), (cudaStream_t)stream>>>(a);
+  int blocks = 0;
+  if (int32_t rc = sampling_grid(&blocks)) return rc;
+  const int tiles_x = (cam->width + kTileW - 1) / kTileW;
+  const int ntiles = tiles_x * ((cam->height + kTileH - 1) / kTileH);
+  char* ws = (char*)workspace;
+  Sched sc;
+  sc.work = (int*)(ws + L.work);
+  sc.order = (int*)(ws + L.order);
+  sc.counts = (int*)(ws + L.small);
+  sc.fill = sc.counts + 32;
+  sc.next = sc.counts + 64;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemsetAsync(sc.counts, 0, 512, st) != cudaSuccess)
+    return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaMemsetAsync failed");
+  k_tile_work<<<(ntiles + 7) / 8, 256, 0, st>>>(a.hash, a.n_sorted, cam->height, cam->width, opt->kernel_size, tiles_x,
+                                                 ntiles, sc);
+  if (int32_t rc = check_launch("k_tile_work")) return rc;
+  k_tile_order<<<(ntiles + 255) / 256 < 148 ? (ntiles + 255) / 256 : 148, 256, 0, st>>>(ntiles, sc);
+  if (int32_t rc = check_launch("k_tile_order")) return rc;
+  k_quick_sampling<<<blocks < ntiles ? blocks : ntiles, kThreads, sizeof(Stage), st>>>(a, sc, tiles_x, ntiles);
   return check_launch("k_quick_sampling");
 }
 

@@ -59,6 +59,8 @@ class ViewPipeline:
         self.pc_idx = torch.empty((self.H, self.W, S, P), dtype=torch.int32, device=dev)
         self.sp_t = torch.empty((self.H, self.W, S), dtype=torch.float32, device=dev)
         self.mask = torch.empty((self.H, self.W, S), dtype=torch.bool, device=dev)
+        self.ws_sample_bytes = L.hp_quick_sampling_workspace_size(self.H, self.W)
+        self.ws_sample = torch.empty(self.ws_sample_bytes, dtype=torch.uint8, device=dev)
 
     def build(self, xyz, cam, stream):
         rc = native.lib().hp_pts2plane(_vp(xyz.data_ptr()), self.n, ctypes.byref(cam), self.sort,
@@ -72,6 +74,7 @@ class ViewPipeline:
                                             _vp(self.sidx.data_ptr()), self.n, _vp(self.hash.data_ptr()),
                                             _vp(self.sp_xyz.data_ptr()), _vp(self.pc_idx.data_ptr()),
                                             _vp(self.sp_t.data_ptr()), _vp(self.mask.data_ptr()),
+                                            _vp(self.ws_sample.data_ptr()), self.ws_sample_bytes,
                                             _vp(stream.cuda_stream))
         native.check(rc, "hp_quick_sampling")
 
@@ -82,5 +85,6 @@ class ViewPipeline:
         return self.sp_xyz, self.pc_idx, self.sp_t, self.mask
 
     # kernels each render() launches (hp_pts2plane: project/count, block sums,
-    # scan, scatter, small-bucket sort, deep-bucket sort; hp_quick_sampling: 1)
-    KERNELS_PER_VIEW = 7
+    # scan, scatter, order, huge-bucket sort; hp_quick_sampling: tile work,
+    # tile order, sampling)
+    KERNELS_PER_VIEW = 9

@@ -30,7 +30,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
 
 # C-ABI symbols declared in include/hashpoint_b200.h
 EXPORTS = ["hp_version", "hp_last_error", "hp_projection_rounding", "hp_pts2plane_workspace_size", "hp_pts2plane",
-           "hp_pts2plane_noalloc", "hp_scatter_hashtable", "hp_quick_sampling", "hp_quick_query_for_nearby_point", "hp_scatter",
+           "hp_pts2plane_noalloc", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling", "hp_quick_query_for_nearby_point", "hp_scatter",
            "hp_ray_directions"]
 
 HP_OK = 0
@@ -133,7 +133,9 @@ def lib():
         L.hp_pts2plane_noalloc.restype = i32
         L.hp_scatter_hashtable.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp, vp]
         L.hp_scatter_hashtable.restype = i32
-        L.hp_quick_sampling.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, vp, vp, vp, vp]
+        L.hp_quick_sampling_workspace_size.argtypes = [i32, i32]
+        L.hp_quick_sampling_workspace_size.restype = sz
+        L.hp_quick_sampling.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, vp, vp, vp, vp, sz, vp]
         L.hp_quick_sampling.restype = i32
         L.hp_quick_query_for_nearby_point.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, i64, vp, vp]
         L.hp_quick_query_for_nearby_point.restype = i32

@@ -134,10 +134,12 @@ def quick_sampling(xyz, c2w, fx, fy, cx, cy, width, height, opt, sorted_point_id
     mask = torch.empty((H, W, S), dtype=torch.bool, device=dev)
     cam = make_camera(c2w=c2w, fx=fx, fy=fy, cx=cx, cy=cy, width=W, height=H)
     o = make_options(opt)
-    rc = native.lib().hp_quick_sampling(_ptr(xyz), xyz.shape[0], ctypes.byref(cam), ctypes.byref(o),
-                                        _ptr(sorted_point_idx), sorted_point_idx.numel(), _ptr(hash_table),
-                                        _ptr(sp_xyz), _ptr(pc_idx),
-                                        _ptr(sp_t), _ptr(mask), _stream(dev))
+    L = native.lib()
+    ws_bytes = L.hp_quick_sampling_workspace_size(H, W)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    rc = L.hp_quick_sampling(_ptr(xyz), xyz.shape[0], ctypes.byref(cam), ctypes.byref(o), _ptr(sorted_point_idx),
+                             sorted_point_idx.numel(), _ptr(hash_table), _ptr(sp_xyz), _ptr(pc_idx), _ptr(sp_t),
+                             _ptr(mask), _ptr(ws), ws_bytes, _stream(dev))
     native.check(rc, "hp_quick_sampling")
     return sp_xyz, pc_idx, sp_t, mask
 

@@ -139,7 +139,12 @@ HP_API int32_t hp_scatter_hashtable(const int32_t* point_idx, const int32_t* poi
  * make the kernel read out of bounds. */
 HP_API int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const hp_camera* cam, const hp_options* opt,
                                  const int32_t* sorted_point_idx, int64_t n_sorted, const int32_t* hash_table,
-                                 float* sp_xyz, int32_t* pc_idx, float* sp_t, uint8_t* mask, hp_stream_t stream);
+                                 float* sp_xyz, int32_t* pc_idx, float* sp_t, uint8_t* mask, void* workspace,
+                                 size_t workspace_bytes, hp_stream_t stream);
+
+/* Scratch bytes hp_quick_sampling needs for an image of this size (its tile
+ * schedule); workspace must be 256-byte aligned. */
+HP_API size_t hp_quick_sampling_workspace_size(int32_t height, int32_t width);
 
 /* Ray query for a list of pixel rays (linear ids v*W+u).  Replaces
  * _C.quick_query_for_nearby_point (epcq/csrc/epcq_render_topk.cu:287-339,

@@ -92,21 +92,30 @@ def _err(L):
                                          (3, 8, 0, 0.01, "num_point_cloud_per_sp"), (3, 8, 8, 0.0, "t_intvl")])
 def test_quick_sampling_rejects_bad_options(L, k, S, P, t, msg):
     p = ctypes.c_void_p(0x1000)
-    rc = L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt(k, S, P, t)), p, 10, p, p, p, p, p, None)
+    rc = L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt(k, S, P, t)), p, 10, p, p, p, p, p, p, 1 << 20,
+                             None)
     assert rc == -1 and msg in _err(L)
 
 
 def test_quick_sampling_rejects_null_and_misaligned(L):
     p = ctypes.c_void_p(0x1000)
-    assert L.hp_quick_sampling(p, 10, None, ctypes.byref(_opt()), p, 10, p, p, p, p, p, None) == -1
-    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, 10, None, p, p, p, p,
+    ws, big = ctypes.c_void_p(0x10000), 1 << 20
+    assert L.hp_quick_sampling(p, 10, None, ctypes.byref(_opt()), p, 10, p, p, p, p, p, ws, big, None) == -1
+    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, 10, None, p, p, p, p, ws, big,
                                None) == -1
     assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, 10, ctypes.c_void_p(0x1004),
-                               p, p, p, p, None) == -1
+                               p, p, p, p, ws, big, None) == -1
     assert "aligned" in _err(L)
-    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam(w=0)), ctypes.byref(_opt()), p, 10, p, p, p, p, p,
+    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam(w=0)), ctypes.byref(_opt()), p, 10, p, p, p, p, p, ws, big,
                                None) == -1
-    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, -1, p, p, p, p, p, None) == -1
+    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, -1, p, p, p, p, p, ws, big,
+                               None) == -1
+    need = L.hp_quick_sampling_workspace_size(8, 8)
+    assert need > 0
+    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, 10, p, p, p, p, p, ws, need - 1,
+                               None) == -2
+    assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, 10, p, p, p, p, p, None, need,
+                               None) == -2
 
 
 def test_pts2plane_checks_workspace(L):
