@@ -408,64 +408,88 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
 }
 
 // Tile scheduling.  A tile's cost grows with the points in its window halo
-// and is very uneven (dense objects vs background), so tiles are handed out
-// heaviest first (a counting sort on log2 of the halo's point count, with
-// halos too large to stage weighted up), to a persistent grid of
-// SMs x resident blocks that takes the next tile from an atomic counter.  The
-// heavy tiles then start first and the light ones fill in around them,
-// instead of a few heavy tiles finishing alone at the end.
+// and is very uneven (dense objects vs background).  Work items are tiles of
+// 8 rows x 32 pixels; a tile whose halo does not fit the stage is split into
+// items of 4, 2 or 1 rows (each staged on its own, so they run concurrently
+// on different SMs).  Items are handed out heaviest first (a counting sort on
+// log2 of the halo's point count; halos still too large to stage weighted up)
+// to a persistent grid of SMs x resident blocks that takes the next item from
+// an atomic counter, so heavy items start first and light ones fill in
+// around them.
 struct Sched {
-  int* work;    // [ntiles] estimated cost
-  int* order;   // [ntiles] tile ids, heaviest first
-  int* counts;  // [32] tiles per cost class
+  int* work;    // [max items] estimated cost
+  int* item;    // [max items] (tile << 8) | (first row << 4) | rows
+  int* order;   // [max items] item indices, heaviest first
+  int* counts;  // [32] items per cost class
   int* fill;    // [32] placement cursors
   int* next;    // [1] next position in `order` to hand out
+  int* n_items; // [1]
 };
 
 __device__ __forceinline__ int cost_class(int w) { return 31 - __clz(w | 1); }
+
+// Points in the window halo of rows [vb, vb + rows) of a tile's columns (one warp).
+__device__ __forceinline__ int halo_points(const int2* __restrict__ hash, int n_sorted, int H, int W, int k, int vb,
+                                           int rows, int u0) {
+  const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
+  const int rv0 = max(0, vb - lo), rv1 = min(H - 1, vb + rows - 1 + hi);
+  const int ru0 = max(0, u0 - lo), ru1 = min(W - 1, u0 + kTileW - 1 + hi);
+  const int nu = ru1 - ru0 + 1, ncells = (rv1 - rv0 + 1) * nu;
+  int sum = 0;
+  for (int c = (threadIdx.x & 31); c < ncells; c += 32) {
+    const int2 rg = bucket_range(__ldg(hash + (size_t)(rv0 + c / nu) * W + ru0 + c % nu), n_sorted);
+    sum += min(rg.y - rg.x, kStageCap + 1);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  return sum;
+}
 
 __global__ void __launch_bounds__(256) k_tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k,
                                                    int tiles_x, int ntiles, Sched sc) {
   const int lane = threadIdx.x & 31;
   const int t = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (t >= ntiles) return;
-  const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
   const int v0 = (t / tiles_x) * kTileH, u0 = (t % tiles_x) * kTileW;
-  const int rv0 = max(0, v0 - lo), rv1 = min(H - 1, v0 + kTileH - 1 + hi);
-  const int ru0 = max(0, u0 - lo), ru1 = min(W - 1, u0 + kTileW - 1 + hi);
-  const int nu = ru1 - ru0 + 1, ncells = (rv1 - rv0 + 1) * nu;
-  int sum = 0;
-  for (int c = lane; c < ncells; c += 32) {
-    const int2 rg = bucket_range(__ldg(hash + (size_t)(rv0 + c / nu) * W + ru0 + c % nu), n_sorted);
-    sum += min(rg.y - rg.x, kStageCap + 1);
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-  if (lane == 0) {
-    const int w = sum > kStageCap ? min(sum, 1 << 26) * 4 : sum;  // unstaged tiles read global memory
-    sc.work[t] = w;
-    atomicAdd(sc.counts + cost_class(w), 1);
+  const int v_end = min(H, v0 + kTileH);
+  // split the tile's rows until each item's halo fits the stage (or is one row)
+  for (int vb = v0; vb < v_end;) {
+    int rows = v_end - vb;
+    int sum = halo_points(hash, n_sorted, H, W, k, vb, rows, u0);
+    while (sum > kStageCap && rows > 1) {
+      rows = (rows + 1) >> 1;
+      sum = halo_points(hash, n_sorted, H, W, k, vb, rows, u0);
+    }
+    if (lane == 0) {
+      const int w = sum > kStageCap ? min(sum, 1 << 26) * 4 : sum;  // unstaged items read global memory
+      const int i = atomicAdd(sc.n_items, 1);
+      sc.work[i] = w;
+      sc.item[i] = (t << 8) | ((vb - v0) << 4) | rows;
+      atomicAdd(sc.counts + cost_class(w), 1);
+    }
+    vb += rows;
   }
 }
 
-__global__ void __launch_bounds__(256) k_tile_order(int ntiles, Sched sc) {
+__global__ void __launch_bounds__(256) k_tile_order(Sched sc) {
   __shared__ int base[32];
   if (threadIdx.x < 32) {
-    int b = 0;  // tiles in heavier classes
+    int b = 0;  // items in heavier classes
     for (int c = 31; c > (int)threadIdx.x; c--) b += sc.counts[c];
     base[threadIdx.x] = b;
   }
   __syncthreads();
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
-    const int c = cost_class(sc.work[t]);
-    sc.order[base[c] + atomicAdd(sc.fill + c, 1)] = t;
+  const int n = *sc.n_items;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = cost_class(sc.work[i]);
+    sc.order[base[c] + atomicAdd(sc.fill + c, 1)] = i;
   }
 }
 
-__device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int v0, int u0) {
+__device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int v0, int rows, int u0) {
   const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
   const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
-  const int rv0 = max(0, v0 - lo), rv1 = min(H - 1, v0 + kTileH - 1 + hi);
+  const int rv0 = max(0, v0 - lo), rv1 = min(H - 1, v0 + rows - 1 + hi);
   const int ru0 = max(0, u0 - lo), ru1 = min(W - 1, u0 + kTileW - 1 + hi);
   const int nu = ru1 - ru0 + 1, ncells = (rv1 - rv0 + 1) * nu;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -535,7 +559,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
   {
     const int pu = u0 + (tid & 31), pv = v0 + (tid >> 5);
     int work = 0;
-    if (pu < W && pv < H) {
+    if (pu < W && pv < H && (tid >> 5) < rows) {
       work = 1;
       for (int l = 0; l < k * k; l++) {
         int vv, uu;
@@ -559,7 +583,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
   }
   const int px = st.order[tid];
   const int u = u0 + (px & 31), v = v0 + (px >> 5);
-  if (u < W && v < H) {
+  if (u < W && v < H && (px >> 5) < rows) {
     if (staged)
       sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v, u);
     else
@@ -568,17 +592,19 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
   __syncthreads();  // the stage is reused by the next tile
 }
 
-__global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a, Sched sc, int tiles_x, int ntiles) {
+__global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a, Sched sc, int tiles_x) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Stage& st = *reinterpret_cast<Stage*>(smem_raw);
   __shared__ int s_next;
+  const int n = *sc.n_items;
   for (;;) {
     if (threadIdx.x == 0) s_next = atomicAdd(sc.next, 1);
     __syncthreads();
     const int i = s_next;
-    if (i >= ntiles) break;
-    const int t = sc.order[i];
-    process_tile(a, st, (t / tiles_x) * kTileH, (t % tiles_x) * kTileW);
+    if (i >= n) break;
+    const int it = sc.item[sc.order[i]];
+    const int t = it >> 8;
+    process_tile(a, st, (t / tiles_x) * kTileH + ((it >> 4) & 15), it & 15, (t % tiles_x) * kTileW);
   }
 }
 
@@ -618,16 +644,19 @@ int32_t sampling_grid(int* blocks) {
 static constexpr size_t align256s(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct SchedLayout {
-  size_t work, order, small, total;
+  size_t work, item, order, small, total;
 };
 
+// up to kTileH items per tile (every row its own item)
 static SchedLayout sched_layout(int64_t H, int64_t W) {
   const int64_t ntiles = ((W + kTileW - 1) / kTileW) * ((H + kTileH - 1) / kTileH);
+  const size_t per = align256s(sizeof(int) * (size_t)(ntiles * kTileH));
   SchedLayout L;
   L.work = 0;
-  L.order = align256s(sizeof(int) * (size_t)ntiles);
-  L.small = L.order + align256s(sizeof(int) * (size_t)ntiles);
-  L.total = L.small + 512;  // counts[32], fill[32], next
+  L.item = per;
+  L.order = 2 * per;
+  L.small = 3 * per;
+  L.total = L.small + 512;  // counts[32], fill[32], next, n_items
   return L;
 }
 
@@ -722,19 +751,21 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   char* ws = (char*)workspace;
   Sched sc;
   sc.work = (int*)(ws + L.work);
+  sc.item = (int*)(ws + L.item);
   sc.order = (int*)(ws + L.order);
   sc.counts = (int*)(ws + L.small);
   sc.fill = sc.counts + 32;
   sc.next = sc.counts + 64;
+  sc.n_items = sc.counts + 65;
   cudaStream_t st = (cudaStream_t)stream;
   if (cudaMemsetAsync(sc.counts, 0, 512, st) != cudaSuccess)
     return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaMemsetAsync failed");
   k_tile_work<<<(ntiles + 7) / 8, 256, 0, st>>>(a.hash, a.n_sorted, cam->height, cam->width, opt->kernel_size, tiles_x,
                                                  ntiles, sc);
   if (int32_t rc = check_launch("k_tile_work")) return rc;
-  k_tile_order<<<(ntiles + 255) / 256 < 148 ? (ntiles + 255) / 256 : 148, 256, 0, st>>>(ntiles, sc);
+  k_tile_order<<<(ntiles + 255) / 256 < 148 ? (ntiles + 255) / 256 : 148, 256, 0, st>>>(sc);
   if (int32_t rc = check_launch("k_tile_order")) return rc;
-  k_quick_sampling<<<blocks < ntiles ? blocks : ntiles, kThreads, sizeof(Stage), st>>>(a, sc, tiles_x, ntiles);
+  k_quick_sampling<<<blocks < ntiles ? blocks : ntiles, kThreads, sizeof(Stage), st>>>(a, sc, tiles_x);
   return check_launch("k_quick_sampling");
 }
 
