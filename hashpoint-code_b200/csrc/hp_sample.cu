@@ -16,8 +16,10 @@
 //   pass B  the same candidates binned by int((t - tmin) / t_intvl); instead of
 //           a 128-bin histogram the thread keeps the 4 smallest distinct bins
 //           (count, distance sum) in registers -- exactly the bins the walk
-//           reaches first -- and re-collects further bins only if the walk
-//           goes past them
+//           reaches first -- and two 128-bit masks of the bins holding one and
+//           at least two points; if the walk goes past the 4 bins, further
+//           rounds collect stats only for the next bins holding >= 2 points
+//           (the only ones the walk uses)
 //   walk    bins with >= 2 points in ascending order: alpha = gamma *
 //           exp(-mean_dist / alpha_g), emit when alpha * T > 1e-3, T -= alpha,
 //           stop when T < 1e-3 or S samples are out
@@ -261,67 +263,16 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
 
   if (!(tmin > tmax)) {
     float transmit = 1.0f;
-    int lo = 0;
-    for (;;) {
-      // pass B: the kBinList smallest distinct bins in [lo, cut) with full stats
-      int lb[kBinList], lc[kBinList];
-      float ls[kBinList];
-#pragma unroll
-      for (int q = 0; q < kBinList; q++) lb[q] = 0x7fffffff, lc[q] = 0, ls[q] = 0.0f;
-      int m = 0, cut = kBins;
-      walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
-        if (__float_as_int(p.w) < 0) return false;
-        float s0, s1, s2;
-        const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
-        const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
-        const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
-        const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
-        if (!within_radius(rt, e0, e1, e2)) return false;
-        const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
-        if (b < lo || b >= cut) return true;
-        if (m == kBinList && b > lb[kBinList - 1]) {
-          cut = b;
-          return true;
-        }
-        const float dist = norm3df(e0, e1, e2);
-        bool found = false;
-#pragma unroll
-        for (int q = 0; q < kBinList; q++)
-          if (q < m && lb[q] == b) {
-            lc[q] += 1;
-            ls[q] = __fadd_rn(ls[q], dist);
-            found = true;
-          }
-        if (found) return true;
-        int pos = 0;
-#pragma unroll
-        for (int q = 0; q < kBinList; q++) pos += (q < m && lb[q] < b) ? 1 : 0;
-        if (m == kBinList) cut = lb[kBinList - 1];
-#pragma unroll
-        for (int q = kBinList - 1; q >= 0; q--) {
-          if (q > pos) {
-            lb[q] = lb[q - 1];
-            lc[q] = lc[q - 1];
-            ls[q] = ls[q - 1];
-          } else if (q == pos) {
-            lb[q] = b;
-            lc[q] = 1;
-            ls[q] = dist;
-          }
-        }
-        m = m < kBinList ? m + 1 : kBinList;
-        return true;
-      });
-      // primary-surface walk (epcq_render_topk.cu:181-204)
-      bool done = false;
+    int lb[kBinList], lc[kBinList];
+    float ls[kBinList];
+    int m = 0;
+    // primary-surface walk over list entries (epcq_render_topk.cu:181-204); returns true when finished
+    auto walk_list = [&]() -> bool {
 #pragma unroll
       for (int q = 0; q < kBinList; q++) {
-        if (q >= m || done) break;
+        if (q >= m) break;
         if (lc[q] < 2) continue;
-        if (transmit < 1e-3f || emitted >= S) {
-          done = true;
-          break;
-        }
+        if (transmit < 1e-3f || emitted >= S) return true;
         const float sdf = __fdiv_rn(ls[q], __fadd_rn((float)lc[q], 1e-6f));
         const float alpha = __fmul_rn(a.opt.gamma, __expf(__fdiv_rn(-sdf, a.opt.alpha_g)));
         const float weight = __fmul_rn(alpha, transmit);
@@ -339,8 +290,121 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
         }
         transmit = __fsub_rn(transmit, alpha);
       }
-      if (done || cut >= kBins) break;
-      lo = cut;
+      return false;
+    };
+
+    // pass B: the kBinList smallest distinct bins with full stats, plus which of
+    // the 128 bins hold one (seen1) and at least two (seen2) kept points
+    unsigned seen1[kBins / 32], seen2[kBins / 32];
+#pragma unroll
+    for (int q = 0; q < kBins / 32; q++) seen1[q] = 0u, seen2[q] = 0u;
+#pragma unroll
+    for (int q = 0; q < kBinList; q++) lb[q] = 0x7fffffff, lc[q] = 0, ls[q] = 0.0f;
+    int cut = kBins;
+    walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
+      if (__float_as_int(p.w) < 0) return false;
+      float s0, s1, s2;
+      const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
+      const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
+      const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
+      const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
+      if (!within_radius(rt, e0, e1, e2)) return false;
+      const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
+      if (b >= kBins) return true;
+      const unsigned bit = 1u << (b & 31);
+#pragma unroll
+      for (int q = 0; q < kBins / 32; q++)
+        if (q == (b >> 5)) {
+          seen2[q] |= seen1[q] & bit;
+          seen1[q] |= bit;
+        }
+      if (b >= cut) return true;
+      if (m == kBinList && b > lb[kBinList - 1]) {
+        cut = b;
+        return true;
+      }
+      const float dist = norm3df(e0, e1, e2);
+      bool found = false;
+#pragma unroll
+      for (int q = 0; q < kBinList; q++)
+        if (q < m && lb[q] == b) {
+          lc[q] += 1;
+          ls[q] = __fadd_rn(ls[q], dist);
+          found = true;
+        }
+      if (found) return true;
+      int pos = 0;
+#pragma unroll
+      for (int q = 0; q < kBinList; q++) pos += (q < m && lb[q] < b) ? 1 : 0;
+      if (m == kBinList) cut = lb[kBinList - 1];
+#pragma unroll
+      for (int q = kBinList - 1; q >= 0; q--) {
+        if (q > pos) {
+          lb[q] = lb[q - 1];
+          lc[q] = lc[q - 1];
+          ls[q] = ls[q - 1];
+        } else if (q == pos) {
+          lb[q] = b;
+          lc[q] = 1;
+          ls[q] = dist;
+        }
+      }
+      m = m < kBinList ? m + 1 : kBinList;
+      return true;
+    });
+    bool done = walk_list();
+    // Further rounds (only when the walk outlives the bins above): stats for the
+    // next kBinList bins holding >= 2 points -- the only bins the walk uses.
+    int lo = cut;
+    while (!done && lo < kBins) {
+      m = 0;
+      unsigned sel[kBins / 32];
+#pragma unroll
+      for (int q = 0; q < kBins / 32; q++) {
+        unsigned mask = seen2[q];
+        if (q * 32 + 32 <= lo) mask = 0u;
+        else if (q * 32 < lo) mask &= ~0u << (lo - q * 32);
+        sel[q] = 0u;
+#pragma unroll
+        for (int e = 0; e < kBinList; e++) {
+          if (m < kBinList && mask) {
+            const int bpos = __ffs(mask) - 1;
+            mask &= mask - 1;
+            sel[q] |= 1u << bpos;
+#pragma unroll
+            for (int f = 0; f < kBinList; f++)
+              if (f == m) lb[f] = q * 32 + bpos, lc[f] = 0, ls[f] = 0.0f;
+            m++;
+          }
+        }
+      }
+      if (m == 0) break;
+      walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
+        if (__float_as_int(p.w) < 0) return false;
+        float s0, s1, s2;
+        const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
+        const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
+        const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
+        const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
+        if (!within_radius(rt, e0, e1, e2)) return false;
+        const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
+        if (b >= kBins) return true;
+        bool hit = false;
+#pragma unroll
+        for (int q = 0; q < kBins / 32; q++)
+          if (q == (b >> 5)) hit = (sel[q] >> (b & 31)) & 1u;
+        if (!hit) return true;
+        const float dist = norm3df(e0, e1, e2);
+#pragma unroll
+        for (int q = 0; q < kBinList; q++)
+          if (q < m && lb[q] == b) {
+            lc[q] += 1;
+            ls[q] = __fadd_rn(ls[q], dist);
+          }
+        return true;
+      });
+      done = walk_list();
+      lo = lb[m - 1] + 1;
     }
   }
 
