@@ -25,11 +25,12 @@
 //           stop when T < 1e-3 or S samples are out
 //   ball    per emitted sample, the reference's 8-entry id buffer over the
 //           whole window (including its quirk that, while the buffer fills, the
-//           tracked "farthest" entry is the nearest one).  Candidates whose
-//           position along the ray is further than radius (+ a rounding
-//           margin orders of magnitude above float error) from the sample are
-//           skipped before the distance is computed: they cannot be within
-//           the radius, so the buffer sees exactly the same sequence.
+//           tracked "farthest" entry is the nearest one), all samples of a ray
+//           in one walk.  Candidates whose position along the ray is further
+//           than radius (+ a rounding margin orders of magnitude above float
+//           error) from a sample are skipped for it before the distance is
+//           computed: they cannot be within the radius, so each buffer sees
+//           exactly the same sequence.
 //
 // Each pass walks the ray's window as one flat candidate sequence, and the
 // tile's rays are ranked by window size before they are handed to threads, so
@@ -59,6 +60,7 @@ constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
 constexpr int kStageCap = 4096;  // staged points per tile (64 KB)
 constexpr int kBinList = 4;      // distinct t-bins collected per candidate pass
 constexpr int kTeReg = 4;        // emitted sample depths kept in registers
+constexpr int kBallPass = 2;     // samples served by one ball-query walk
 
 struct SampleArgs {
   const float* __restrict__ xyz;
@@ -408,58 +410,85 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
     }
   }
 
-  // per-sample point selection (epcq_render_topk.cu:10-81)
+  // per-sample point selection (epcq_render_topk.cu:10-81).  One walk over the
+  // window serves up to kBallPass samples: each candidate's position along the
+  // ray is compared with every sample's reach (samples are in ascending t), and
+  // only candidates within a sample's reach get the exact distance.  The
+  // per-sample buffers live in a small local array touched only on hits.
   const float omax = fmaxf(fabsf(r.o[0]), fmaxf(fabsf(r.o[1]), fabsf(r.o[2])));
-  for (int s = 0; s < emitted; s++) {
-    float ts = o_t[s];
+  for (int s0 = 0; s0 < emitted; s0 += kBallPass) {
+    const int ns = min(kBallPass, emitted - s0);
+    float ts[kBallPass], reach[kBallPass], spx[kBallPass], spy[kBallPass], spz[kBallPass], maxd[kBallPass];
+    float bd[kBallPass][kBallBuf];
+    int bi[kBallPass][kBallBuf], bsize[kBallPass], maxi[kBallPass];
 #pragma unroll
-    for (int e = 0; e < kTeReg; e++)
-      if (e == s) ts = te[e];
-    const float sx = __fmaf_rn(ts, r.d[0], r.o[0]), sy = __fmaf_rn(ts, r.d[1], r.o[1]),
-                sz = __fmaf_rn(ts, r.d[2], r.o[2]);
-    // |position along the ray - ts| beyond this cannot be within the radius
-    const float reach = radius * 1.001f + 1e-5f * (1.0f + fabsf(ts) + omax);
-    float bd[kBallBuf];
-    int bi[kBallBuf];
+    for (int q = 0; q < kBallPass; q++) {
+      float t = 0.0f;
+      if (q < ns) {
+        t = o_t[s0 + q];
 #pragma unroll
-    for (int q = 0; q < kBallBuf; q++) bd[q] = 0.0f, bi[q] = -1;
-    int bsize = 0, maxi = 0;
-    float maxd = 1e3f;
+        for (int e = 0; e < kTeReg; e++)
+          if (e == s0 + q) t = te[e];
+      }
+      ts[q] = t;
+      // |position along the ray - t| beyond this cannot be within the radius
+      reach[q] = q < ns ? radius * 1.001f + 1e-5f * (1.0f + fabsf(t) + omax) : -1.0f;
+      spx[q] = __fmaf_rn(t, r.d[0], r.o[0]);
+      spy[q] = __fmaf_rn(t, r.d[1], r.o[1]);
+      spz[q] = __fmaf_rn(t, r.d[2], r.o[2]);
+      bsize[q] = 0;
+      maxi[q] = 0;
+      maxd[q] = 1e3f;
+#pragma unroll
+      for (int e = 0; e < kBallBuf; e++) bd[q][e] = 0.0f, bi[q][e] = -1;
+    }
+    const float t_first = ts[0] - reach[0], t_last = ts[ns - 1 > 0 ? 1 : 0] + reach[ns - 1 > 0 ? 1 : 0];
     walk_window(a, src, v, u, 0x7fffffff, [&](const float4& p) -> bool {
       const int id = __float_as_int(p.w);
       if (id < 0) return false;
       const float along = dot3(p.x - r.o[0], p.y - r.o[1], p.z - r.o[2], r.d[0], r.d[1], r.d[2]);
-      if (fabsf(along - ts) > reach) return false;
-      const float dist = norm3df(__fsub_rn(sx, p.x), __fsub_rn(sy, p.y), __fsub_rn(sz, p.z));
-      if (!(dist < radius)) return false;
-      if (bsize < kBallBuf) {
+      if (along < t_first || along > t_last) return false;
 #pragma unroll
-        for (int q = 0; q < kBallBuf; q++)
-          if (q == bsize) bd[q] = dist, bi[q] = id;
-        if (maxd > dist) {
-          maxd = dist;
-          maxi = bsize;
-        }
-        bsize++;
-      } else if (dist < maxd) {
+      for (int q = 0; q < kBallPass; q++) {
+        if (!(fabsf(along - ts[q]) <= reach[q])) continue;
+        const float dist = norm3df(__fsub_rn(spx[q], p.x), __fsub_rn(spy[q], p.y), __fsub_rn(spz[q], p.z));
+        if (!(dist < radius)) continue;
+        if (bsize[q] < kBallBuf) {
 #pragma unroll
-        for (int q = 0; q < kBallBuf; q++)
-          if (q == maxi) bd[q] = dist, bi[q] = id;
-        maxd = dist;
-#pragma unroll
-        for (int q = 0; q < kBallBuf; q++)
-          if (bd[q] > maxd) {
-            maxd = bd[q];
-            maxi = q;
+          for (int e = 0; e < kBallBuf; e++)
+            if (e == bsize[q]) bd[q][e] = dist, bi[q][e] = id;
+          if (maxd[q] > dist) {
+            maxd[q] = dist;
+            maxi[q] = bsize[q];
           }
+          bsize[q]++;
+        } else if (dist < maxd[q]) {
+#pragma unroll
+          for (int e = 0; e < kBallBuf; e++)
+            if (e == maxi[q]) bd[q][e] = dist, bi[q][e] = id;
+          float md = dist;
+          int mi = maxi[q];
+#pragma unroll
+          for (int e = 0; e < kBallBuf; e++)
+            if (bd[q][e] > md) {
+              md = bd[q][e];
+              mi = e;
+            }
+          maxd[q] = md;
+          maxi[q] = mi;
+        }
       }
       return false;
     });
-    int* row = o_idx + (size_t)s * P;
 #pragma unroll
-    for (int q = 0; q < kBallBuf; q++)
-      if (q < P) row[q] = q < bsize ? bi[q] : -1;
-    if (P > kBallBuf) fill_run(row + kBallBuf, P - kBallBuf, -1);
+    for (int q = 0; q < kBallPass; q++) {
+      if (q >= ns) break;
+      int* row = o_idx + (size_t)(s0 + q) * P;
+#pragma unroll
+      for (int e = 0; e < kBallBuf; e++)
+        if (e < P) row[e] = e < bsize[q] ? bi[q][e] : -1;
+      if (P > kBallBuf) fill_run(row + kBallBuf, P - kBallBuf, -1);
+    }
   }
 
   // defaults for the slots nothing was emitted into
