@@ -16,10 +16,8 @@
 //   pass B  the same candidates binned by int((t - tmin) / t_intvl); instead of
 //           a 128-bin histogram the thread keeps the 4 smallest distinct bins
 //           (count, distance sum) in registers -- exactly the bins the walk
-//           reaches first -- and two 128-bit masks of the bins holding one and
-//           at least two points; if the walk goes past the 4 bins, further
-//           rounds collect stats only for the next bins holding >= 2 points
-//           (the only ones the walk uses)
+//           reaches first -- and re-collects further bins only if the walk
+//           goes past them
 //   walk    bins with >= 2 points in ascending order: alpha = gamma *
 //           exp(-mean_dist / alpha_g), emit when alpha * T > 1e-3, T -= alpha,
 //           stop when T < 1e-3 or S samples are out
@@ -61,6 +59,7 @@ constexpr int kStageCap = 4096;  // staged points per tile (64 KB)
 constexpr int kBinList = 4;      // distinct t-bins collected per candidate pass
 constexpr int kTeReg = 4;        // emitted sample depths kept in registers
 constexpr int kBallPass = 2;     // samples served by one ball-query walk
+constexpr int kHeavyWindow = 256; // rays with more window candidates are served by a whole warp
 
 struct SampleArgs {
   const float* __restrict__ xyz;
@@ -265,16 +264,67 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
 
   if (!(tmin > tmax)) {
     float transmit = 1.0f;
-    int lb[kBinList], lc[kBinList];
-    float ls[kBinList];
-    int m = 0;
-    // primary-surface walk over list entries (epcq_render_topk.cu:181-204); returns true when finished
-    auto walk_list = [&]() -> bool {
+    int lo = 0;
+    for (;;) {
+      // pass B: the kBinList smallest distinct bins in [lo, cut) with full stats
+      int lb[kBinList], lc[kBinList];
+      float ls[kBinList];
+#pragma unroll
+      for (int q = 0; q < kBinList; q++) lb[q] = 0x7fffffff, lc[q] = 0, ls[q] = 0.0f;
+      int m = 0, cut = kBins;
+      walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
+        if (__float_as_int(p.w) < 0) return false;
+        float s0, s1, s2;
+        const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
+        const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
+        const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
+        const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
+        if (!within_radius(rt, e0, e1, e2)) return false;
+        const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
+        if (b < lo || b >= cut) return true;
+        if (m == kBinList && b > lb[kBinList - 1]) {
+          cut = b;
+          return true;
+        }
+        const float dist = norm3df(e0, e1, e2);
+        bool found = false;
+#pragma unroll
+        for (int q = 0; q < kBinList; q++)
+          if (q < m && lb[q] == b) {
+            lc[q] += 1;
+            ls[q] = __fadd_rn(ls[q], dist);
+            found = true;
+          }
+        if (found) return true;
+        int pos = 0;
+#pragma unroll
+        for (int q = 0; q < kBinList; q++) pos += (q < m && lb[q] < b) ? 1 : 0;
+        if (m == kBinList) cut = lb[kBinList - 1];
+#pragma unroll
+        for (int q = kBinList - 1; q >= 0; q--) {
+          if (q > pos) {
+            lb[q] = lb[q - 1];
+            lc[q] = lc[q - 1];
+            ls[q] = ls[q - 1];
+          } else if (q == pos) {
+            lb[q] = b;
+            lc[q] = 1;
+            ls[q] = dist;
+          }
+        }
+        m = m < kBinList ? m + 1 : kBinList;
+        return true;
+      });
+      // primary-surface walk (epcq_render_topk.cu:181-204)
+      bool done = false;
 #pragma unroll
       for (int q = 0; q < kBinList; q++) {
-        if (q >= m) break;
+        if (q >= m || done) break;
         if (lc[q] < 2) continue;
-        if (transmit < 1e-3f || emitted >= S) return true;
+        if (transmit < 1e-3f || emitted >= S) {
+          done = true;
+          break;
+        }
         const float sdf = __fdiv_rn(ls[q], __fadd_rn((float)lc[q], 1e-6f));
         const float alpha = __fmul_rn(a.opt.gamma, __expf(__fdiv_rn(-sdf, a.opt.alpha_g)));
         const float weight = __fmul_rn(alpha, transmit);
@@ -292,121 +342,8 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
         }
         transmit = __fsub_rn(transmit, alpha);
       }
-      return false;
-    };
-
-    // pass B: the kBinList smallest distinct bins with full stats, plus which of
-    // the 128 bins hold one (seen1) and at least two (seen2) kept points
-    unsigned seen1[kBins / 32], seen2[kBins / 32];
-#pragma unroll
-    for (int q = 0; q < kBins / 32; q++) seen1[q] = 0u, seen2[q] = 0u;
-#pragma unroll
-    for (int q = 0; q < kBinList; q++) lb[q] = 0x7fffffff, lc[q] = 0, ls[q] = 0.0f;
-    int cut = kBins;
-    walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
-      if (__float_as_int(p.w) < 0) return false;
-      float s0, s1, s2;
-      const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
-      const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
-      const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
-      const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
-      if (!within_radius(rt, e0, e1, e2)) return false;
-      const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
-      if (b >= kBins) return true;
-      const unsigned bit = 1u << (b & 31);
-#pragma unroll
-      for (int q = 0; q < kBins / 32; q++)
-        if (q == (b >> 5)) {
-          seen2[q] |= seen1[q] & bit;
-          seen1[q] |= bit;
-        }
-      if (b >= cut) return true;
-      if (m == kBinList && b > lb[kBinList - 1]) {
-        cut = b;
-        return true;
-      }
-      const float dist = norm3df(e0, e1, e2);
-      bool found = false;
-#pragma unroll
-      for (int q = 0; q < kBinList; q++)
-        if (q < m && lb[q] == b) {
-          lc[q] += 1;
-          ls[q] = __fadd_rn(ls[q], dist);
-          found = true;
-        }
-      if (found) return true;
-      int pos = 0;
-#pragma unroll
-      for (int q = 0; q < kBinList; q++) pos += (q < m && lb[q] < b) ? 1 : 0;
-      if (m == kBinList) cut = lb[kBinList - 1];
-#pragma unroll
-      for (int q = kBinList - 1; q >= 0; q--) {
-        if (q > pos) {
-          lb[q] = lb[q - 1];
-          lc[q] = lc[q - 1];
-          ls[q] = ls[q - 1];
-        } else if (q == pos) {
-          lb[q] = b;
-          lc[q] = 1;
-          ls[q] = dist;
-        }
-      }
-      m = m < kBinList ? m + 1 : kBinList;
-      return true;
-    });
-    bool done = walk_list();
-    // Further rounds (only when the walk outlives the bins above): stats for the
-    // next kBinList bins holding >= 2 points -- the only bins the walk uses.
-    int lo = cut;
-    while (!done && lo < kBins) {
-      m = 0;
-      unsigned sel[kBins / 32];
-#pragma unroll
-      for (int q = 0; q < kBins / 32; q++) {
-        unsigned mask = seen2[q];
-        if (q * 32 + 32 <= lo) mask = 0u;
-        else if (q * 32 < lo) mask &= ~0u << (lo - q * 32);
-        sel[q] = 0u;
-#pragma unroll
-        for (int e = 0; e < kBinList; e++) {
-          if (m < kBinList && mask) {
-            const int bpos = __ffs(mask) - 1;
-            mask &= mask - 1;
-            sel[q] |= 1u << bpos;
-#pragma unroll
-            for (int f = 0; f < kBinList; f++)
-              if (f == m) lb[f] = q * 32 + bpos, lc[f] = 0, ls[f] = 0.0f;
-            m++;
-          }
-        }
-      }
-      if (m == 0) break;
-      walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
-        if (__float_as_int(p.w) < 0) return false;
-        float s0, s1, s2;
-        const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
-        const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
-        const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
-        const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
-        if (!within_radius(rt, e0, e1, e2)) return false;
-        const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
-        if (b >= kBins) return true;
-        bool hit = false;
-#pragma unroll
-        for (int q = 0; q < kBins / 32; q++)
-          if (q == (b >> 5)) hit = (sel[q] >> (b & 31)) & 1u;
-        if (!hit) return true;
-        const float dist = norm3df(e0, e1, e2);
-#pragma unroll
-        for (int q = 0; q < kBinList; q++)
-          if (q < m && lb[q] == b) {
-            lc[q] += 1;
-            ls[q] = __fadd_rn(ls[q], dist);
-          }
-        return true;
-      });
-      done = walk_list();
-      lo = lb[m - 1] + 1;
+      if (done || cut >= kBins) break;
+      lo = cut;
     }
   }
 
@@ -498,6 +435,284 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
     fill_run(o_m + emitted, S - emitted, (uint8_t)0);
     fill_run(o_idx + (size_t)emitted * P, (S - emitted) * P, -1);
   }
+}
+
+// Warp-cooperative sample_ray for rays with large windows.  The 32 lanes take
+// consecutive candidates of a window cell; everything order-dependent -- the
+// 48-per-cell cap (ballot ranks), bin sums (added one by one in candidate
+// order through shuffles) and the 8-entry ball buffers (fed accepted
+// candidates in order) -- reproduces sample_ray exactly.  A tile hands its
+// heaviest rays to this routine so that no single thread walks a huge window
+// serially while the rest of the GPU waits for it.
+template <class Src>
+__device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& src, int v, int u) {
+  const unsigned kAll = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
+  const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
+  const int ray = v * W + u;
+  const int S = a.opt.S, P = a.opt.P;
+  const float radius = a.opt.radius;
+  Ray r;
+  make_ray(a.cam.c2w, a.cam.fx, a.cam.fy, a.cam.cx, a.cam.cy, u, v, r);
+  const bool unit = r.dd == 1.0f;
+  const RadiusTest rt = make_radius_test(radius);
+
+  // window cells in the reference's order (rows, then columns, clamped)
+  auto cells = [&](auto&& f) {
+    for (int dv = -lo; dv <= hi; dv++) {
+      const int vv = min(max(v + dv, 0), H - 1);
+      for (int du = -lo; du <= hi; du++) {
+        const int2 rg = src.range(a, vv, min(max(u + du, 0), W - 1));
+        f(rg.x, rg.y);
+      }
+    }
+  };
+  // one lane's candidate: kept (radius test) with its t and offset from the ray
+  auto eval = [&](int j, int ce, float& t, float& e0, float& e1, float& e2) -> bool {
+    if (j >= ce) return false;
+    const float4 p = src.fetch(a, j);
+    if (__float_as_int(p.w) < 0) return false;
+    float s0, s1, s2;
+    t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
+    e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
+    e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
+    e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
+    return within_radius(rt, e0, e1, e2);
+  };
+
+  // pass A: tmin / tmax
+  float tmin = 1e3f, tmax = -1e3f;
+  cells([&](int cb, int ce) {
+    int run = 0;
+    for (int j0 = cb; j0 < ce && run < kKeptPerCell; j0 += 32) {
+      float t = 0.f, e0, e1, e2;
+      const bool kept = eval(j0 + lane, ce, t, e0, e1, e2);
+      const unsigned m = __ballot_sync(kAll, kept);
+      if (kept && run + __popc(m & below) < kKeptPerCell) {
+        if (tmin > t) tmin = t;
+        if (tmax < t) tmax = t;
+      }
+      run += __popc(m);
+    }
+  });
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float a0 = __shfl_xor_sync(kAll, tmin, o), a1 = __shfl_xor_sync(kAll, tmax, o);
+    if (tmin > a0) tmin = a0;
+    if (tmax < a1) tmax = a1;
+  }
+
+  float* o_xyz = a.sp_xyz + (size_t)ray * S * 3;
+  float* o_t = a.sp_t + (size_t)ray * S;
+  uint8_t* o_m = a.mask + (size_t)ray * S;
+  int* o_idx = a.pc_idx + (size_t)ray * S * P;
+  int emitted = 0;
+  float te[kTeReg];
+#pragma unroll
+  for (int q = 0; q < kTeReg; q++) te[q] = 0.0f;
+
+  if (!(tmin > tmax)) {
+    // pass B: which bins hold >= 2 kept points (the only ones the walk uses)
+    unsigned s1[kBins / 32], s2[kBins / 32];
+#pragma unroll
+    for (int q = 0; q < kBins / 32; q++) s1[q] = 0u, s2[q] = 0u;
+    cells([&](int cb, int ce) {
+      int run = 0;
+      for (int j0 = cb; j0 < ce && run < kKeptPerCell; j0 += 32) {
+        float t = 0.f, e0, e1, e2;
+        const bool kept = eval(j0 + lane, ce, t, e0, e1, e2);
+        const unsigned m = __ballot_sync(kAll, kept);
+        if (kept && run + __popc(m & below) < kKeptPerCell) {
+          const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
+          if (b < kBins) {
+            const unsigned bit = 1u << (b & 31);
+#pragma unroll
+            for (int q = 0; q < kBins / 32; q++)
+              if (q == (b >> 5)) {
+                s2[q] |= s1[q] & bit;
+                s1[q] |= bit;
+              }
+          }
+        }
+        run += __popc(m);
+      }
+    });
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int q = 0; q < kBins / 32; q++) {
+        const unsigned o1 = __shfl_xor_sync(kAll, s1[q], o), o2 = __shfl_xor_sync(kAll, s2[q], o);
+        s2[q] = s2[q] | o2 | (s1[q] & o1);
+        s1[q] |= o1;
+      }
+    }
+    // walk over the bins holding >= 2 points, ascending
+    float transmit = 1.0f;
+    int from = 0;
+    for (;;) {
+      int bstar = kBins;
+#pragma unroll
+      for (int q = kBins / 32 - 1; q >= 0; q--) {
+        unsigned mask = s2[q];
+        if (q * 32 + 32 <= from) mask = 0u;
+        else if (q * 32 < from) mask &= ~0u << (from - q * 32);
+        if (mask) bstar = q * 32 + __ffs(mask) - 1;
+      }
+      if (bstar >= kBins) break;
+      if (transmit < 1e-3f || emitted >= S) break;
+      int cnt = 0;
+      float sum = 0.0f;
+      cells([&](int cb, int ce) {
+        int run = 0;
+        for (int j0 = cb; j0 < ce && run < kKeptPerCell; j0 += 32) {
+          float t = 0.f, e0 = 0.f, e1 = 0.f, e2 = 0.f;
+          const bool kept = eval(j0 + lane, ce, t, e0, e1, e2);
+          const unsigned m = __ballot_sync(kAll, kept);
+          bool member = false;
+          float dist = 0.0f;
+          if (kept && run + __popc(m & below) < kKeptPerCell &&
+              __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl)) == bstar) {
+            member = true;
+            dist = norm3df(e0, e1, e2);
+          }
+          unsigned mm = __ballot_sync(kAll, member);
+          while (mm) {
+            const int l = __ffs(mm) - 1;
+            mm &= mm - 1;
+            sum = __fadd_rn(sum, __shfl_sync(kAll, dist, l));
+            cnt++;
+          }
+          run += __popc(m);
+        }
+      });
+      const float sdf = __fdiv_rn(sum, __fadd_rn((float)cnt, 1e-6f));
+      const float alpha = __fmul_rn(a.opt.gamma, __expf(__fdiv_rn(-sdf, a.opt.alpha_g)));
+      const float weight = __fmul_rn(alpha, transmit);
+      if (weight > 1e-3f) {
+        const float t = __fmaf_rn((float)bstar, a.opt.t_intvl, tmin);
+        if (lane == 0) {
+          o_xyz[emitted * 3 + 0] = __fmaf_rn(t, r.d[0], r.o[0]);
+          o_xyz[emitted * 3 + 1] = __fmaf_rn(t, r.d[1], r.o[1]);
+          o_xyz[emitted * 3 + 2] = __fmaf_rn(t, r.d[2], r.o[2]);
+          o_t[emitted] = t;
+          o_m[emitted] = 1;
+        }
+#pragma unroll
+        for (int e = 0; e < kTeReg; e++)
+          if (e == emitted) te[e] = t;
+        emitted++;
+      }
+      transmit = __fsub_rn(transmit, alpha);
+      from = bstar + 1;
+    }
+  }
+  __syncwarp();
+
+  // per-sample point selection, two samples per walk, buffers fed in order
+  const float omax = fmaxf(fabsf(r.o[0]), fmaxf(fabsf(r.o[1]), fabsf(r.o[2])));
+  for (int s0 = 0; s0 < emitted; s0 += kBallPass) {
+    const int ns = min(kBallPass, emitted - s0);
+    float ts[kBallPass], reach[kBallPass], spx[kBallPass], spy[kBallPass], spz[kBallPass], maxd[kBallPass];
+    float bd[kBallPass][kBallBuf];
+    int bi[kBallPass][kBallBuf], bsize[kBallPass], maxi[kBallPass];
+#pragma unroll
+    for (int q = 0; q < kBallPass; q++) {
+      float t = 0.0f;
+      if (q < ns) {
+        t = o_t[s0 + q];
+#pragma unroll
+        for (int e = 0; e < kTeReg; e++)
+          if (e == s0 + q) t = te[e];
+      }
+      ts[q] = t;
+      reach[q] = q < ns ? radius * 1.001f + 1e-5f * (1.0f + fabsf(t) + omax) : -1.0f;
+      spx[q] = __fmaf_rn(t, r.d[0], r.o[0]);
+      spy[q] = __fmaf_rn(t, r.d[1], r.o[1]);
+      spz[q] = __fmaf_rn(t, r.d[2], r.o[2]);
+      bsize[q] = 0;
+      maxi[q] = 0;
+      maxd[q] = 1e3f;
+#pragma unroll
+      for (int e = 0; e < kBallBuf; e++) bd[q][e] = 0.0f, bi[q][e] = -1;
+    }
+    cells([&](int cb, int ce) {
+      for (int j0 = cb; j0 < ce; j0 += 32) {
+        const int j = j0 + lane;
+        float dq[kBallPass];
+        bool hq[kBallPass];
+        int id = -1;
+#pragma unroll
+        for (int q = 0; q < kBallPass; q++) dq[q] = 0.0f, hq[q] = false;
+        if (j < ce) {
+          const float4 p = src.fetch(a, j);
+          id = __float_as_int(p.w);
+          if (id >= 0) {
+            const float along = dot3(p.x - r.o[0], p.y - r.o[1], p.z - r.o[2], r.d[0], r.d[1], r.d[2]);
+#pragma unroll
+            for (int q = 0; q < kBallPass; q++)
+              if (fabsf(along - ts[q]) <= reach[q]) {
+                dq[q] = norm3df(__fsub_rn(spx[q], p.x), __fsub_rn(spy[q], p.y), __fsub_rn(spz[q], p.z));
+                hq[q] = dq[q] < radius;
+              }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kBallPass; q++) {
+          unsigned mm = __ballot_sync(kAll, hq[q]);
+          while (mm) {
+            const int l = __ffs(mm) - 1;
+            mm &= mm - 1;
+            const float dist = __shfl_sync(kAll, dq[q], l);
+            const int cid = __shfl_sync(kAll, id, l);
+            if (bsize[q] < kBallBuf) {
+#pragma unroll
+              for (int e = 0; e < kBallBuf; e++)
+                if (e == bsize[q]) bd[q][e] = dist, bi[q][e] = cid;
+              if (maxd[q] > dist) {
+                maxd[q] = dist;
+                maxi[q] = bsize[q];
+              }
+              bsize[q]++;
+            } else if (dist < maxd[q]) {
+#pragma unroll
+              for (int e = 0; e < kBallBuf; e++)
+                if (e == maxi[q]) bd[q][e] = dist, bi[q][e] = cid;
+              float md = dist;
+              int mi = maxi[q];
+#pragma unroll
+              for (int e = 0; e < kBallBuf; e++)
+                if (bd[q][e] > md) {
+                  md = bd[q][e];
+                  mi = e;
+                }
+              maxd[q] = md;
+              maxi[q] = mi;
+            }
+          }
+        }
+      }
+    });
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < kBallPass; q++) {
+        if (q >= ns) break;
+        int* row = o_idx + (size_t)(s0 + q) * P;
+#pragma unroll
+        for (int e = 0; e < kBallBuf; e++)
+          if (e < P) row[e] = e < bsize[q] ? bi[q][e] : -1;
+        if (P > kBallBuf) fill_run(row + kBallBuf, P - kBallBuf, -1);
+      }
+    }
+  }
+  if (lane == 0 && emitted < S) {
+    fill_run(o_xyz + emitted * 3, (S - emitted) * 3, 0.0f);
+    fill_run(o_t + emitted, S - emitted, 0.0f);
+    fill_run(o_m + emitted, S - emitted, (uint8_t)0);
+    fill_run(o_idx + (size_t)emitted * P, (S - emitted) * P, -1);
+  }
+  __syncwarp();
 }
 
 // Tile scheduling.  A tile's cost grows with the points in its window halo
@@ -648,7 +863,10 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
   }
 
   // Rank the tile's rays by their window's candidate count so each warp gets
-  // rays of similar work (the flat loops then diverge little).
+  // rays of similar work (the flat loops then diverge little).  Rays whose
+  // window exceeds kHeavyWindow candidates come first and are served by whole
+  // warps (sample_ray_warp); the rest get one thread each.
+  int nheavy = 0;
   {
     const int pu = u0 + (tid & 31), pv = v0 + (tid >> 5);
     int work = 0;
@@ -663,7 +881,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
     }
     int* work_flat = reinterpret_cast<int*>(st.work);
     work_flat[tid] = (min(work, 0x7fffff) << 8) | tid;
-    __syncthreads();
+    nheavy = __syncthreads_count(work > kHeavyWindow);
     const int mine = work_flat[tid];
     int rank = 0;
 #pragma unroll 8
@@ -674,13 +892,24 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
     st.order[rank] = tid;
     __syncthreads();
   }
-  const int px = st.order[tid];
-  const int u = u0 + (px & 31), v = v0 + (px >> 5);
-  if (u < W && v < H && (px >> 5) < rows) {
+  for (int h = tid >> 5; h < nheavy; h += kThreads / 32) {
+    const int px = st.order[h];
     if (staged)
-      sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v, u);
+      sample_ray_warp(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
     else
-      sample_ray(a, SrcGlobal{}, v, u);
+      sample_ray_warp(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
+  }
+  // light rays: the lightest go to warp 0, which may also have served a heavy ray
+  const int li = kThreads - 1 - tid;
+  if (li >= nheavy) {
+    const int px = st.order[li];
+    const int u = u0 + (px & 31), v = v0 + (px >> 5);
+    if (u < W && v < H && (px >> 5) < rows) {
+      if (staged)
+        sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v, u);
+      else
+        sample_ray(a, SrcGlobal{}, v, u);
+    }
   }
   __syncthreads();  // the stage is reused by the next tile
 }
