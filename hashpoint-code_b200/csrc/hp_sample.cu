@@ -56,10 +56,18 @@ constexpr int kThreads = kTileW * kTileH;
 constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
 constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
 constexpr int kStageCap = 4096;  // staged points per tile (64 KB)
+#ifndef HP_SPLIT_WORK
+#define HP_SPLIT_WORK 4096
+#endif
+constexpr int kSplitWork = HP_SPLIT_WORK;  // tiles whose halo holds more points are split into row bands
 constexpr int kBinList = 4;      // distinct t-bins collected per candidate pass
 constexpr int kTeReg = 4;        // emitted sample depths kept in registers
 constexpr int kBallPass = 2;     // samples served by one ball-query walk
-constexpr int kHeavyWindow = 256; // rays with more window candidates are served by a whole warp
+#ifndef HP_HEAVY_WINDOW
+#define HP_HEAVY_WINDOW 320
+#endif
+constexpr int kHeavyWindow = HP_HEAVY_WINDOW;  // rays with more window candidates get a whole warp
+constexpr int kWalkBatch = 4;    // bins whose sums one walk pass of a warp-served ray gathers
 
 struct SampleArgs {
   const float* __restrict__ xyz;
@@ -82,6 +90,7 @@ struct Stage {
   int off[kHaloMax + 1];   // staged offset of each halo cell, exclusive prefix
   int start[kHaloMax];     // the cell's first index in sorted_point_idx
   int warp_tot[kThreads / 32];
+  int next_unit;            // next work unit of the tile (see process_tile)
 };
 
 // Clipped bucket range of a hash entry: [x, x + count) within [0, n_sorted).
@@ -437,20 +446,30 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
   }
 }
 
-// Warp-cooperative sample_ray for rays with large windows.  The 32 lanes take
-// consecutive candidates of a window cell; everything order-dependent -- the
-// 48-per-cell cap (ballot ranks), bin sums (added one by one in candidate
-// order through shuffles) and the 8-entry ball buffers (fed accepted
-// candidates in order) -- reproduces sample_ray exactly.  A tile hands its
-// heaviest rays to this routine so that no single thread walks a huge window
-// serially while the rest of the GPU waits for it.
+// Lanes [lo, hi) of a warp as a bit mask (0 <= lo <= hi <= 32).
+__device__ __forceinline__ unsigned lane_span(int lo, int hi) {
+  const unsigned below_hi = hi >= 32 ? 0xffffffffu : (1u << hi) - 1u;
+  const unsigned below_lo = lo >= 32 ? 0xffffffffu : (1u << lo) - 1u;
+  return below_hi & ~below_lo;
+}
+
+// Warp-cooperative sample_ray.  The ray's k*k window cells (reference order:
+// rows, then columns, clamped) are concatenated into one candidate sequence:
+// lane c < k*k holds cell c's range and its exclusive prefix, and each chunk
+// of 32 consecutive candidates is spread over the lanes, every lane finding its
+// cell by a binary search over the prefixes (shuffles).  Everything
+// order-dependent reproduces sample_ray exactly: the 48-per-cell cap from
+// ballot ranks plus a per-cell carry, bin sums added one candidate at a time
+// in sequence order, and the 8-entry ball buffers fed hits in sequence order.
+// A ray costs about ceil(candidates / 32) chunks per pass, so heavy rays finish
+// in a fraction of the time one thread would need for them.
 template <class Src>
 __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& src, int v, int u) {
   const unsigned kAll = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
   const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
-  const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
+  const int lo = ((k + 1) >> 1) - 1;
   const int ray = v * W + u;
   const int S = a.opt.S, P = a.opt.P;
   const float radius = a.opt.radius;
@@ -459,20 +478,43 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
   const bool unit = r.dd == 1.0f;
   const RadiusTest rt = make_radius_test(radius);
 
-  // window cells in the reference's order (rows, then columns, clamped)
-  auto cells = [&](auto&& f) {
-    for (int dv = -lo; dv <= hi; dv++) {
-      const int vv = min(max(v + dv, 0), H - 1);
-      for (int du = -lo; du <= hi; du++) {
-        const int2 rg = src.range(a, vv, min(max(u + du, 0), W - 1));
-        f(rg.x, rg.y);
-      }
+  // lane c < k*k: cell c's first index and count; exclusive prefix over cells
+  int cbase = 0, ccnt = 0;
+  if (lane < k * k) {
+    const int q = lane / k;
+    const int vv = min(max(v + q - lo, 0), H - 1), uu = min(max(u + (lane - q * k) - lo, 0), W - 1);
+    const int2 rg = src.range(a, vv, uu);
+    cbase = rg.x;
+    ccnt = rg.y - rg.x;
+  }
+  int cpre = ccnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kAll, cpre, o);
+    if (lane >= o) cpre += t;
+  }
+  const int total = __shfl_sync(kAll, cpre, 31);
+  cpre -= ccnt;
+  const bool capped = __any_sync(kAll, ccnt > kKeptPerCell);
+
+  // body(j0, valid, idx, cell, pc) per lane and chunk: candidate j0 + lane of
+  // the sequence, its index for src.fetch, its cell and the cell's first j
+  auto chunks = [&](auto&& body) {
+    for (int j0 = 0; j0 < total; j0 += 32) {
+      const int j = j0 + lane;
+      int c = 0;
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1)
+        if (__shfl_sync(kAll, cpre, c + s) <= j) c += s;
+      const int pc = __shfl_sync(kAll, cpre, c);
+      const int idx = __shfl_sync(kAll, cbase, c) + (j - pc);
+      body(j0, j < total, idx, c, pc);
     }
   };
-  // one lane's candidate: kept (radius test) with its t and offset from the ray
-  auto eval = [&](int j, int ce, float& t, float& e0, float& e1, float& e2) -> bool {
-    if (j >= ce) return false;
-    const float4 p = src.fetch(a, j);
+  // the candidate's t and offset from the ray; true when within the radius
+  auto eval = [&](bool valid, int idx, float& t, float& e0, float& e1, float& e2) -> bool {
+    if (!valid) return false;
+    const float4 p = src.fetch(a, idx);
     if (__float_as_int(p.w) < 0) return false;
     float s0, s1, s2;
     t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
@@ -481,22 +523,31 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
     e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
     return within_radius(rt, e0, e1, e2);
   };
+  // kept candidates that are among the first 48 kept of their cell; `carry`
+  // (lane c's copy is cell c's) counts a cell's kept candidates of earlier chunks
+  auto accept = [&](bool kept, int j0, int cell, int pc, int& carry) -> bool {
+    if (!capped) return kept;
+    const unsigned m = __ballot_sync(kAll, kept);
+    const int before = __shfl_sync(kAll, carry, cell) + __popc(m & below & ~lane_span(0, max(pc - j0, 0)));
+    carry += __popc(m & lane_span(min(max(cpre - j0, 0), 32), min(max(cpre + ccnt - j0, 0), 32)));
+    return kept && before < kKeptPerCell;
+  };
+  auto bin_of = [&](float t, float tmin) {
+    return __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
+  };
 
   // pass A: tmin / tmax
   float tmin = 1e3f, tmax = -1e3f;
-  cells([&](int cb, int ce) {
-    int run = 0;
-    for (int j0 = cb; j0 < ce && run < kKeptPerCell; j0 += 32) {
+  {
+    int carry = 0;
+    chunks([&](int j0, bool valid, int idx, int cell, int pc) {
       float t = 0.f, e0, e1, e2;
-      const bool kept = eval(j0 + lane, ce, t, e0, e1, e2);
-      const unsigned m = __ballot_sync(kAll, kept);
-      if (kept && run + __popc(m & below) < kKeptPerCell) {
+      if (accept(eval(valid, idx, t, e0, e1, e2), j0, cell, pc, carry)) {
         if (tmin > t) tmin = t;
         if (tmax < t) tmax = t;
       }
-      run += __popc(m);
-    }
-  });
+    });
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const float a0 = __shfl_xor_sync(kAll, tmin, o), a1 = __shfl_xor_sync(kAll, tmax, o);
@@ -518,14 +569,12 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
     unsigned s1[kBins / 32], s2[kBins / 32];
 #pragma unroll
     for (int q = 0; q < kBins / 32; q++) s1[q] = 0u, s2[q] = 0u;
-    cells([&](int cb, int ce) {
-      int run = 0;
-      for (int j0 = cb; j0 < ce && run < kKeptPerCell; j0 += 32) {
+    {
+      int carry = 0;
+      chunks([&](int j0, bool valid, int idx, int cell, int pc) {
         float t = 0.f, e0, e1, e2;
-        const bool kept = eval(j0 + lane, ce, t, e0, e1, e2);
-        const unsigned m = __ballot_sync(kAll, kept);
-        if (kept && run + __popc(m & below) < kKeptPerCell) {
-          const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
+        if (accept(eval(valid, idx, t, e0, e1, e2), j0, cell, pc, carry)) {
+          const int b = bin_of(t, tmin);
           if (b < kBins) {
             const unsigned bit = 1u << (b & 31);
 #pragma unroll
@@ -536,9 +585,8 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
               }
           }
         }
-        run += __popc(m);
-      }
-    });
+      });
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -548,69 +596,93 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
         s1[q] |= o1;
       }
     }
-    // walk over the bins holding >= 2 points, ascending
-    float transmit = 1.0f;
-    int from = 0;
-    for (;;) {
-      int bstar = kBins;
+    // first bin >= from holding >= 2 points (kBins if none)
+    auto next_bin = [&](int from) {
+      int b = kBins;
 #pragma unroll
       for (int q = kBins / 32 - 1; q >= 0; q--) {
-        unsigned mask = s2[q];
-        if (q * 32 + 32 <= from) mask = 0u;
-        else if (q * 32 < from) mask &= ~0u << (from - q * 32);
-        if (mask) bstar = q * 32 + __ffs(mask) - 1;
+        unsigned m = s2[q];
+        if (q * 32 + 32 <= from)
+          m = 0u;
+        else if (q * 32 < from)
+          m &= ~0u << (from - q * 32);
+        if (m) b = q * 32 + __ffs(m) - 1;
       }
-      if (bstar >= kBins) break;
-      if (transmit < 1e-3f || emitted >= S) break;
-      int cnt = 0;
-      float sum = 0.0f;
-      cells([&](int cb, int ce) {
-        int run = 0;
-        for (int j0 = cb; j0 < ce && run < kKeptPerCell; j0 += 32) {
-          float t = 0.f, e0 = 0.f, e1 = 0.f, e2 = 0.f;
-          const bool kept = eval(j0 + lane, ce, t, e0, e1, e2);
-          const unsigned m = __ballot_sync(kAll, kept);
-          bool member = false;
-          float dist = 0.0f;
-          if (kept && run + __popc(m & below) < kKeptPerCell &&
-              __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl)) == bstar) {
-            member = true;
-            dist = norm3df(e0, e1, e2);
-          }
-          unsigned mm = __ballot_sync(kAll, member);
+      return b;
+    };
+    // walk: the bins' sums are gathered kWalkBatch bins per pass, in ascending order
+    float transmit = 1.0f;
+    int from = 0;
+    bool done = false;
+    while (!done) {
+      int bb[kWalkBatch];
+      int nb = 0;
+#pragma unroll
+      for (int q = 0; q < kWalkBatch; q++) {
+        bb[q] = next_bin(q == 0 ? from : bb[q - 1] + 1);
+        nb += bb[q] < kBins ? 1 : 0;
+      }
+      if (nb == 0) break;
+      float bsum[kWalkBatch];
+      int bcnt[kWalkBatch];
+#pragma unroll
+      for (int q = 0; q < kWalkBatch; q++) bsum[q] = 0.0f, bcnt[q] = 0;
+      int carry = 0;
+      chunks([&](int j0, bool valid, int idx, int cell, int pc) {
+        float t = 0.f, e0 = 0.f, e1 = 0.f, e2 = 0.f;
+        int mine = -1;
+        float dist = 0.0f;
+        if (accept(eval(valid, idx, t, e0, e1, e2), j0, cell, pc, carry)) {
+          const int b = bin_of(t, tmin);
+#pragma unroll
+          for (int q = 0; q < kWalkBatch; q++)
+            if (bb[q] == b) mine = q;
+          if (mine >= 0) dist = norm3df(e0, e1, e2);
+        }
+#pragma unroll
+        for (int q = 0; q < kWalkBatch; q++) {
+          unsigned mm = __ballot_sync(kAll, mine == q);
           while (mm) {
             const int l = __ffs(mm) - 1;
             mm &= mm - 1;
-            sum = __fadd_rn(sum, __shfl_sync(kAll, dist, l));
-            cnt++;
+            bsum[q] = __fadd_rn(bsum[q], __shfl_sync(kAll, dist, l));
+            bcnt[q]++;
           }
-          run += __popc(m);
         }
       });
-      const float sdf = __fdiv_rn(sum, __fadd_rn((float)cnt, 1e-6f));
-      const float alpha = __fmul_rn(a.opt.gamma, __expf(__fdiv_rn(-sdf, a.opt.alpha_g)));
-      const float weight = __fmul_rn(alpha, transmit);
-      if (weight > 1e-3f) {
-        const float t = __fmaf_rn((float)bstar, a.opt.t_intvl, tmin);
-        if (lane == 0) {
-          o_xyz[emitted * 3 + 0] = __fmaf_rn(t, r.d[0], r.o[0]);
-          o_xyz[emitted * 3 + 1] = __fmaf_rn(t, r.d[1], r.o[1]);
-          o_xyz[emitted * 3 + 2] = __fmaf_rn(t, r.d[2], r.o[2]);
-          o_t[emitted] = t;
-          o_m[emitted] = 1;
-        }
 #pragma unroll
-        for (int e = 0; e < kTeReg; e++)
-          if (e == emitted) te[e] = t;
-        emitted++;
+      for (int q = 0; q < kWalkBatch; q++) {
+        if (q >= nb) break;
+        if (transmit < 1e-3f || emitted >= S) {
+          done = true;
+          break;
+        }
+        const float sdf = __fdiv_rn(bsum[q], __fadd_rn((float)bcnt[q], 1e-6f));
+        const float alpha = __fmul_rn(a.opt.gamma, __expf(__fdiv_rn(-sdf, a.opt.alpha_g)));
+        const float weight = __fmul_rn(alpha, transmit);
+        if (weight > 1e-3f) {
+          const float t = __fmaf_rn((float)bb[q], a.opt.t_intvl, tmin);
+          if (lane == 0) {
+            o_xyz[emitted * 3 + 0] = __fmaf_rn(t, r.d[0], r.o[0]);
+            o_xyz[emitted * 3 + 1] = __fmaf_rn(t, r.d[1], r.o[1]);
+            o_xyz[emitted * 3 + 2] = __fmaf_rn(t, r.d[2], r.o[2]);
+            o_t[emitted] = t;
+            o_m[emitted] = 1;
+          }
+#pragma unroll
+          for (int e = 0; e < kTeReg; e++)
+            if (e == emitted) te[e] = t;
+          emitted++;
+        }
+        transmit = __fsub_rn(transmit, alpha);
       }
-      transmit = __fsub_rn(transmit, alpha);
-      from = bstar + 1;
+      if (nb < kWalkBatch) break;
+      from = bb[kWalkBatch - 1] + 1;
     }
   }
   __syncwarp();
 
-  // per-sample point selection, two samples per walk, buffers fed in order
+  // per-sample point selection, two samples per pass, buffers fed hits in order
   const float omax = fmaxf(fabsf(r.o[0]), fmaxf(fabsf(r.o[1]), fabsf(r.o[2])));
   for (int s0 = 0; s0 < emitted; s0 += kBallPass) {
     const int ns = min(kBallPass, emitted - s0);
@@ -637,80 +709,78 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
 #pragma unroll
       for (int e = 0; e < kBallBuf; e++) bd[q][e] = 0.0f, bi[q][e] = -1;
     }
-    cells([&](int cb, int ce) {
-      for (int j0 = cb; j0 < ce; j0 += 32) {
-        const int j = j0 + lane;
-        float dq[kBallPass];
-        bool hq[kBallPass];
-        int id = -1;
+    chunks([&](int, bool valid, int idx, int, int) {
+      float dq[kBallPass];
+      bool hq[kBallPass];
+      int id = -1;
 #pragma unroll
-        for (int q = 0; q < kBallPass; q++) dq[q] = 0.0f, hq[q] = false;
-        if (j < ce) {
-          const float4 p = src.fetch(a, j);
-          id = __float_as_int(p.w);
-          if (id >= 0) {
-            const float along = dot3(p.x - r.o[0], p.y - r.o[1], p.z - r.o[2], r.d[0], r.d[1], r.d[2]);
+      for (int q = 0; q < kBallPass; q++) dq[q] = 0.0f, hq[q] = false;
+      if (valid) {
+        const float4 p = src.fetch(a, idx);
+        id = __float_as_int(p.w);
+        if (id >= 0) {
+          const float along = dot3(p.x - r.o[0], p.y - r.o[1], p.z - r.o[2], r.d[0], r.d[1], r.d[2]);
 #pragma unroll
-            for (int q = 0; q < kBallPass; q++)
-              if (fabsf(along - ts[q]) <= reach[q]) {
-                dq[q] = norm3df(__fsub_rn(spx[q], p.x), __fsub_rn(spy[q], p.y), __fsub_rn(spz[q], p.z));
-                hq[q] = dq[q] < radius;
-              }
-          }
-        }
-#pragma unroll
-        for (int q = 0; q < kBallPass; q++) {
-          unsigned mm = __ballot_sync(kAll, hq[q]);
-          while (mm) {
-            const int l = __ffs(mm) - 1;
-            mm &= mm - 1;
-            const float dist = __shfl_sync(kAll, dq[q], l);
-            const int cid = __shfl_sync(kAll, id, l);
-            if (bsize[q] < kBallBuf) {
-#pragma unroll
-              for (int e = 0; e < kBallBuf; e++)
-                if (e == bsize[q]) bd[q][e] = dist, bi[q][e] = cid;
-              if (maxd[q] > dist) {
-                maxd[q] = dist;
-                maxi[q] = bsize[q];
-              }
-              bsize[q]++;
-            } else if (dist < maxd[q]) {
-#pragma unroll
-              for (int e = 0; e < kBallBuf; e++)
-                if (e == maxi[q]) bd[q][e] = dist, bi[q][e] = cid;
-              float md = dist;
-              int mi = maxi[q];
-#pragma unroll
-              for (int e = 0; e < kBallBuf; e++)
-                if (bd[q][e] > md) {
-                  md = bd[q][e];
-                  mi = e;
-                }
-              maxd[q] = md;
-              maxi[q] = mi;
+          for (int q = 0; q < kBallPass; q++)
+            if (fabsf(along - ts[q]) <= reach[q]) {
+              dq[q] = norm3df(__fsub_rn(spx[q], p.x), __fsub_rn(spy[q], p.y), __fsub_rn(spz[q], p.z));
+              hq[q] = dq[q] < radius;
             }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kBallPass; q++) {
+        unsigned mm = __ballot_sync(kAll, hq[q]);
+        while (mm) {
+          const int l = __ffs(mm) - 1;
+          mm &= mm - 1;
+          const float dist = __shfl_sync(kAll, dq[q], l);
+          const int cid = __shfl_sync(kAll, id, l);
+          if (bsize[q] < kBallBuf) {
+#pragma unroll
+            for (int e = 0; e < kBallBuf; e++)
+              if (e == bsize[q]) bd[q][e] = dist, bi[q][e] = cid;
+            if (maxd[q] > dist) {
+              maxd[q] = dist;
+              maxi[q] = bsize[q];
+            }
+            bsize[q]++;
+          } else if (dist < maxd[q]) {
+#pragma unroll
+            for (int e = 0; e < kBallBuf; e++)
+              if (e == maxi[q]) bd[q][e] = dist, bi[q][e] = cid;
+            float md = dist;
+            int mi = maxi[q];
+#pragma unroll
+            for (int e = 0; e < kBallBuf; e++)
+              if (bd[q][e] > md) {
+                md = bd[q][e];
+                mi = e;
+              }
+            maxd[q] = md;
+            maxi[q] = mi;
           }
         }
       }
     });
-    if (lane == 0) {
 #pragma unroll
-      for (int q = 0; q < kBallPass; q++) {
-        if (q >= ns) break;
-        int* row = o_idx + (size_t)(s0 + q) * P;
+    for (int q = 0; q < kBallPass; q++) {
+      if (q >= ns) break;
+      int* row = o_idx + (size_t)(s0 + q) * P;
+      int val = -1;
 #pragma unroll
-        for (int e = 0; e < kBallBuf; e++)
-          if (e < P) row[e] = e < bsize[q] ? bi[q][e] : -1;
-        if (P > kBallBuf) fill_run(row + kBallBuf, P - kBallBuf, -1);
-      }
+      for (int e = 0; e < kBallBuf; e++)
+        if (e == lane && e < bsize[q]) val = bi[q][e];
+      if (lane < min(P, kBallBuf)) row[lane] = val;
+      if (P > kBallBuf)
+        for (int e = kBallBuf + lane; e < P; e += 32) row[e] = -1;
     }
   }
-  if (lane == 0 && emitted < S) {
-    fill_run(o_xyz + emitted * 3, (S - emitted) * 3, 0.0f);
-    fill_run(o_t + emitted, S - emitted, 0.0f);
-    fill_run(o_m + emitted, S - emitted, (uint8_t)0);
-    fill_run(o_idx + (size_t)emitted * P, (S - emitted) * P, -1);
+  if (emitted < S) {
+    const int n3 = (S - emitted) * 3, n1 = S - emitted, np = (S - emitted) * P;
+    for (int e = lane; e < n3; e += 32) o_xyz[emitted * 3 + e] = 0.0f;
+    for (int e = lane; e < n1; e += 32) o_t[emitted + e] = 0.0f, o_m[emitted + e] = 0;
+    for (int e = lane; e < np; e += 32) o_idx[(size_t)emitted * P + e] = -1;
   }
   __syncwarp();
 }
@@ -760,16 +830,20 @@ __global__ void __launch_bounds__(256) k_tile_work(const int2* __restrict__ hash
   if (t >= ntiles) return;
   const int v0 = (t / tiles_x) * kTileH, u0 = (t % tiles_x) * kTileW;
   const int v_end = min(H, v0 + kTileH);
-  // split the tile's rows until each item's halo fits the stage (or is one row)
+  // split the tile's rows until each item's halo holds at most kSplitWork
+  // points (so no item runs much longer than the average) or is one row
   for (int vb = v0; vb < v_end;) {
     int rows = v_end - vb;
     int sum = halo_points(hash, n_sorted, H, W, k, vb, rows, u0);
-    while (sum > kStageCap && rows > 1) {
+    while (sum > kSplitWork && rows > 1) {
       rows = (rows + 1) >> 1;
       sum = halo_points(hash, n_sorted, H, W, k, vb, rows, u0);
     }
     if (lane == 0) {
-      const int w = sum > kStageCap ? min(sum, 1 << 26) * 4 : sum;  // unstaged items read global memory
+      // cost estimate: the halo's points scaled by the share of its rows that
+      // hold the item's rays; unstaged items (global memory reads) count 4x
+      const int c = (int)(((long long)min(sum, 1 << 24) * rows * kTileH) / (rows + k - 1));
+      const int w = sum > kStageCap ? c * 4 : c;
       const int i = atomicAdd(sc.n_items, 1);
       sc.work[i] = w;
       sc.item[i] = (t << 8) | ((vb - v0) << 4) | rows;
@@ -862,11 +936,13 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
     __syncthreads();
   }
 
-  // Rank the tile's rays by their window's candidate count so each warp gets
-  // rays of similar work (the flat loops then diverge little).  Rays whose
-  // window exceeds kHeavyWindow candidates come first and are served by whole
-  // warps (sample_ray_warp); the rest get one thread each.
-  int nheavy = 0;
+  // Rank the tile's rays by their window's candidate count.  The warps then
+  // pull work units heaviest first: one unit per ray with more than
+  // kHeavyWindow candidates (served by the whole warp, sample_ray_warp), then
+  // groups of 32 consecutive ranks (one ray per thread, similar loop lengths).
+  // Warps that finish early take the next unit, so a tile ends within about
+  // one unit of its total work divided by its warps.
+  int nheavy, nvalid;
   {
     const int pu = u0 + (tid & 31), pv = v0 + (tid >> 5);
     int work = 0;
@@ -881,7 +957,9 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
     }
     int* work_flat = reinterpret_cast<int*>(st.work);
     work_flat[tid] = (min(work, 0x7fffff) << 8) | tid;
+    if (tid == 0) st.next_unit = 0;
     nheavy = __syncthreads_count(work > kHeavyWindow);
+    nvalid = __syncthreads_count(work > 0);
     const int mine = work_flat[tid];
     int rank = 0;
 #pragma unroll 8
@@ -892,23 +970,26 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
     st.order[rank] = tid;
     __syncthreads();
   }
-  for (int h = tid >> 5; h < nheavy; h += kThreads / 32) {
-    const int px = st.order[h];
-    if (staged)
-      sample_ray_warp(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
-    else
-      sample_ray_warp(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
-  }
-  // light rays: the lightest go to warp 0, which may also have served a heavy ray
-  const int li = kThreads - 1 - tid;
-  if (li >= nheavy) {
-    const int px = st.order[li];
-    const int u = u0 + (px & 31), v = v0 + (px >> 5);
-    if (u < W && v < H && (px >> 5) < rows) {
+  for (;;) {
+    int unit = 0;
+    if (lane == 0) unit = atomicAdd(&st.next_unit, 1);
+    unit = __shfl_sync(0xffffffffu, unit, 0);
+    if (unit < nheavy) {
+      const int px = st.order[unit];
       if (staged)
-        sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v, u);
+        sample_ray_warp(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
       else
-        sample_ray(a, SrcGlobal{}, v, u);
+        sample_ray_warp(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
+      continue;
+    }
+    const int r0 = nheavy + (unit - nheavy) * 32;
+    if (r0 >= nvalid) break;
+    if (r0 + lane < nvalid) {
+      const int px = st.order[r0 + lane];
+      if (staged)
+        sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
+      else
+        sample_ray(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
     }
   }
   __syncthreads();  // the stage is reused by the next tile
