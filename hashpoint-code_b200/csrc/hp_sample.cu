@@ -937,11 +937,12 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
   }
 
   // Rank the tile's rays by their window's candidate count.  The warps then
-  // pull work units heaviest first: one unit per ray with more than
-  // kHeavyWindow candidates (served by the whole warp, sample_ray_warp), then
-  // groups of 32 consecutive ranks (one ray per thread, similar loop lengths).
-  // Warps that finish early take the next unit, so a tile ends within about
-  // one unit of its total work divided by its warps.
+  // pull work units, longest first: groups of 32 consecutive ranks below
+  // kHeavyWindow candidates (one ray per thread, similar loop lengths; a group
+  // runs as long as its heaviest ray), then one unit per heavier ray (served by
+  // the whole warp, sample_ray_warp, in about a 32nd of that time).  Warps that
+  // finish early take the next unit, so a tile ends within about one short
+  // unit of its total work divided by its warps.
   int nheavy, nvalid;
   {
     const int pu = u0 + (tid & 31), pv = v0 + (tid >> 5);
@@ -970,27 +971,29 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
     st.order[rank] = tid;
     __syncthreads();
   }
+  const int ngroups = (nvalid - nheavy + 31) >> 5;
   for (;;) {
     int unit = 0;
     if (lane == 0) unit = atomicAdd(&st.next_unit, 1);
     unit = __shfl_sync(0xffffffffu, unit, 0);
-    if (unit < nheavy) {
-      const int px = st.order[unit];
-      if (staged)
-        sample_ray_warp(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
-      else
-        sample_ray_warp(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
+    if (unit < ngroups) {
+      const int rk = nheavy + unit * 32 + lane;
+      if (rk < nvalid) {
+        const int px = st.order[rk];
+        if (staged)
+          sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
+        else
+          sample_ray(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
+      }
       continue;
     }
-    const int r0 = nheavy + (unit - nheavy) * 32;
-    if (r0 >= nvalid) break;
-    if (r0 + lane < nvalid) {
-      const int px = st.order[r0 + lane];
-      if (staged)
-        sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
-      else
-        sample_ray(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
-    }
+    const int h = unit - ngroups;
+    if (h >= nheavy) break;
+    const int px = st.order[h];
+    if (staged)
+      sample_ray_warp(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
+    else
+      sample_ray_warp(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
   }
   __syncthreads();  // the stage is reused by the next tile
 }
