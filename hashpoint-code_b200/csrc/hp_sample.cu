@@ -67,6 +67,8 @@ constexpr int kBallPass = 2;     // samples served by one ball-query walk
 #define HP_HEAVY_WINDOW 320
 #endif
 constexpr int kHeavyWindow = HP_HEAVY_WINDOW;  // rays with more window candidates get a whole warp
+constexpr int kClasses = 64;     // window-size classes used to group a tile's rays
+constexpr int kClassWidth = kHeavyWindow / 40 > 0 ? kHeavyWindow / 40 : 1;  // candidates per class
 constexpr int kWalkBatch = 4;    // bins whose sums one walk pass of a warp-served ray gathers
 
 struct SampleArgs {
@@ -85,8 +87,9 @@ struct SampleArgs {
 
 struct Stage {
   float4 cand[kStageCap];  // x, y, z, id (as int bits; -1 = invalid id)
-  int4 work[kThreads / 4]; // per pixel of the tile: (window candidates << 8) | pixel
-  int order[kThreads];     // pixel each thread processes, most work first
+  int cls[kClasses];        // rays per window-size class
+  int cls_base[kClasses];   // first rank of each class
+  int order[kThreads];      // pixel of each rank, heaviest class first
   int off[kHaloMax + 1];   // staged offset of each halo cell, exclusive prefix
   int start[kHaloMax];     // the cell's first index in sorted_point_idx
   int warp_tot[kThreads / 32];
@@ -936,8 +939,9 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
     __syncthreads();
   }
 
-  // Rank the tile's rays by their window's candidate count.  The warps then
-  // pull work units, longest first: groups of 32 consecutive ranks below
+  // Group the tile's rays by their window's candidate count (a counting sort
+  // over size classes; the order within a class does not affect any output).
+  // The warps then pull work units, longest first: groups of 32 consecutive ranks below
   // kHeavyWindow candidates (one ray per thread, similar loop lengths; a group
   // runs as long as its heaviest ray), then one unit per heavier ray (served by
   // the whole warp, sample_ray_warp, in about a 32nd of that time).  Warps that
@@ -946,29 +950,47 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
   int nheavy, nvalid;
   {
     const int pu = u0 + (tid & 31), pv = v0 + (tid >> 5);
-    int work = 0;
+    int T = -1;  // window candidates; -1: no ray at this pixel
     if (pu < W && pv < H && (tid >> 5) < rows) {
-      work = 1;
-      for (int l = 0; l < k * k; l++) {
-        int vv, uu;
-        window_cell(pv, pu, k, H, W, l, vv, uu);
-        const int2 rg = staged ? SrcStaged{&st, rv0, ru0, nu}.range(a, vv, uu) : SrcGlobal{}.range(a, vv, uu);
-        work += rg.y - rg.x;
+      T = 0;
+      if (staged && pu - lo >= 0 && pu + hi <= W - 1) {
+        // unclamped columns: each window row is a run of k consecutive halo cells
+        for (int dv = -lo; dv <= hi; dv++) {
+          const int c0 = (min(max(pv + dv, 0), H - 1) - rv0) * nu + (pu - lo - ru0);
+          T += st.off[c0 + k] - st.off[c0];
+        }
+      } else {
+        for (int l = 0; l < k * k; l++) {
+          int vv, uu;
+          window_cell(pv, pu, k, H, W, l, vv, uu);
+          const int2 rg = staged ? SrcStaged{&st, rv0, ru0, nu}.range(a, vv, uu) : SrcGlobal{}.range(a, vv, uu);
+          T += rg.y - rg.x;
+        }
       }
     }
-    int* work_flat = reinterpret_cast<int*>(st.work);
-    work_flat[tid] = (min(work, 0x7fffff) << 8) | tid;
+    if (tid < kClasses) st.cls[tid] = 0;
     if (tid == 0) st.next_unit = 0;
-    nheavy = __syncthreads_count(work > kHeavyWindow);
-    nvalid = __syncthreads_count(work > 0);
-    const int mine = work_flat[tid];
-    int rank = 0;
-#pragma unroll 8
-    for (int q = 0; q < kThreads / 4; q++) {
-      const int4 w4 = st.work[q];
-      rank += (w4.x > mine) + (w4.y > mine) + (w4.z > mine) + (w4.w > mine);
+    __syncthreads();
+    // class 0: warp-served rays; then light rays by descending window size; last: no ray
+    const int c = T < 0 ? kClasses - 1
+                        : (T > kHeavyWindow ? 0 : 1 + min(kClasses - 3, (kHeavyWindow - T) / kClassWidth));
+    const int local = atomicAdd(&st.cls[c], 1);
+    __syncthreads();
+    if (tid < 32) {
+      const int n0 = st.cls[2 * tid], n1 = st.cls[2 * tid + 1];
+      int incl = n0 + n1;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (tid >= o) incl += t;
+      }
+      st.cls_base[2 * tid] = incl - n0 - n1;
+      st.cls_base[2 * tid + 1] = incl - n1;
     }
-    st.order[rank] = tid;
+    __syncthreads();
+    st.order[st.cls_base[c] + local] = tid;
+    nheavy = st.cls[0];
+    nvalid = kThreads - st.cls[kClasses - 1];
     __syncthreads();
   }
   const int ngroups = (nvalid - nheavy + 31) >> 5;
