@@ -228,6 +228,33 @@ __device__ __forceinline__ bool within_radius(const RadiusTest& rt, float e0, fl
   return norm3df(e0, e1, e2) < rt.r;
 }
 
+// t-bin index int((t - tmin) / t_intvl) of a kept candidate (x = t - tmin >= 0).
+// y = x * RN(1 / t_intvl) is within 3.1 * 2^-24 * q of the quotient q and of
+// its rounding RN(q), so when y widened by 2^-21 relative on both sides
+// truncates to one integer, that integer is int(RN(q)); otherwise (a bin
+// edge within a few ulps) the division is done exactly.
+struct BinDiv {
+  float intvl, inv;
+  bool fast;
+};
+
+__device__ __forceinline__ BinDiv make_bin_div(float intvl) {
+  BinDiv bd;
+  bd.intvl = intvl;
+  bd.inv = __frcp_rn(intvl);
+  bd.fast = intvl > 0.0f && bd.inv < 0x1p100f && intvl < 0x1p100f;
+  return bd;
+}
+
+__device__ __forceinline__ int bin_index(const BinDiv& bd, float x) {
+  if (bd.fast) {
+    const float y = __fmul_rn(x, bd.inv);
+    const int lo = __float2int_rz(__fmul_rn(y, 1.0f - 0x1p-21f));
+    if (lo == __float2int_rz(__fmul_rn(y, 1.0f + 0x1p-21f))) return lo;
+  }
+  return __float2int_rz(__fdiv_rn(x, bd.intvl));
+}
+
 // PointRayInterset's t (cuda_util.cuh:227); dividing by d.d == 1 is exact, so it is skipped then.
 __device__ __forceinline__ float ray_t(const Ray& r, bool unit, float px, float py, float pz, float& s0, float& s1,
                                       float& s2) {
@@ -275,6 +302,7 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
   for (int q = 0; q < kTeReg; q++) te[q] = 0.0f;
 
   if (!(tmin > tmax)) {
+    const BinDiv bdiv = make_bin_div(a.opt.t_intvl);
     float transmit = 1.0f;
     int lo = 0;
     for (;;) {
@@ -292,7 +320,7 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
         const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
         const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
         if (!within_radius(rt, e0, e1, e2)) return false;
-        const int b = __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
+        const int b = bin_index(bdiv, __fsub_rn(t, tmin));
         if (b < lo || b >= cut) return true;
         if (m == kBinList && b > lb[kBinList - 1]) {
           cut = b;
@@ -535,8 +563,9 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
     carry += __popc(m & lane_span(min(max(cpre - j0, 0), 32), min(max(cpre + ccnt - j0, 0), 32)));
     return kept && before < kKeptPerCell;
   };
+  const BinDiv bdiv = make_bin_div(a.opt.t_intvl);
   auto bin_of = [&](float t, float tmin) {
-    return __float2int_rz(__fdiv_rn(__fsub_rn(t, tmin), a.opt.t_intvl));
+    return bin_index(bdiv, __fsub_rn(t, tmin));
   };
 
   // pass A: tmin / tmax
