@@ -60,7 +60,10 @@ constexpr int kStageCap = 4096;  // staged points per tile (64 KB)
 #define HP_SPLIT_WORK 4096
 #endif
 constexpr int kSplitWork = HP_SPLIT_WORK;  // tiles whose halo holds more points are split into row bands
-constexpr int kBinList = 4;      // distinct t-bins collected per candidate pass
+#ifndef HP_BIN_LIST
+#define HP_BIN_LIST 6
+#endif
+constexpr int kBinList = HP_BIN_LIST;  // distinct t-bins collected per candidate pass
 constexpr int kTeReg = 4;        // emitted sample depths kept in registers
 constexpr int kBallPass = 2;     // samples served by one ball-query walk
 #ifndef HP_HEAVY_WINDOW
@@ -431,18 +434,16 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
         const float dist = norm3df(__fsub_rn(spx[q], p.x), __fsub_rn(spy[q], p.y), __fsub_rn(spz[q], p.z));
         if (!(dist < radius)) continue;
         if (bsize[q] < kBallBuf) {
-#pragma unroll
-          for (int e = 0; e < kBallBuf; e++)
-            if (e == bsize[q]) bd[q][e] = dist, bi[q][e] = id;
+          bd[q][bsize[q]] = dist;  // one indexed store into the local-memory buffer
+          bi[q][bsize[q]] = id;
           if (maxd[q] > dist) {
             maxd[q] = dist;
             maxi[q] = bsize[q];
           }
           bsize[q]++;
         } else if (dist < maxd[q]) {
-#pragma unroll
-          for (int e = 0; e < kBallBuf; e++)
-            if (e == maxi[q]) bd[q][e] = dist, bi[q][e] = id;
+          bd[q][maxi[q]] = dist;
+          bi[q][maxi[q]] = id;
           float md = dist;
           int mi = maxi[q];
 #pragma unroll
