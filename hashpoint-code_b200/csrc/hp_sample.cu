@@ -55,11 +55,8 @@ constexpr int kTileH = 8;    // rows per block
 constexpr int kThreads = kTileW * kTileH;
 constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
 constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
-constexpr int kStageCap = 4096;  // staged points per tile (64 KB)
-#ifndef HP_SPLIT_WORK
-#define HP_SPLIT_WORK 4096
-#endif
-constexpr int kSplitWork = HP_SPLIT_WORK;  // tiles whose halo holds more points are split into row bands
+constexpr int kStageCap = 3584;  // staged points per tile (56 KB)
+constexpr int kSplitWork = kStageCap;  // tiles whose halo holds more points are split into row bands
 #ifndef HP_BIN_LIST
 #define HP_BIN_LIST 6
 #endif
@@ -70,6 +67,7 @@ constexpr int kBallPass = 2;     // samples served by one ball-query walk
 #define HP_HEAVY_WINDOW 320
 #endif
 constexpr int kHeavyWindow = HP_HEAVY_WINDOW;  // rays with more window candidates get a whole warp
+constexpr int kMaskWords = (kHeavyWindow + 31) / 32;  // kept-candidate mask of a thread-served ray
 constexpr int kClasses = 64;     // window-size classes used to group a tile's rays
 constexpr int kClassWidth = kHeavyWindow / 40 > 0 ? kHeavyWindow / 40 : 1;  // candidates per class
 constexpr int kWalkBatch = 4;    // bins whose sums one walk pass of a warp-served ray gathers
@@ -97,7 +95,10 @@ struct Stage {
   int start[kHaloMax];     // the cell's first index in sorted_point_idx
   int warp_tot[kThreads / 32];
   int next_unit;            // next work unit of the tile (see process_tile)
+  unsigned kept[kMaskWords][kThreads];  // per thread: window positions pass A accepted
 };
+// three CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
+static_assert(3 * (sizeof(Stage) + 16 + 1024) <= 228 * 1024, "stage too large for three CTAs per SM");
 
 // Clipped bucket range of a hash entry: [x, x + count) within [0, n_sorted).
 __device__ __forceinline__ int2 bucket_range(int2 h, int n_sorted) {
@@ -186,6 +187,64 @@ __device__ __forceinline__ void walk_window(const SampleArgs& a, const Src& src,
   }
 }
 
+// Staged tiles, unclamped window columns: the same visit as walk_window's
+// fast path, also passing each candidate's position f in the window's
+// candidate sequence (window rows concatenated, entries in stage order).
+template <class Body>
+__device__ __forceinline__ void walk_rows(const SampleArgs& a, const SrcStaged& src, int v, int u, int cap,
+                                          Body&& body) {
+  const int H = a.cam.height, k = a.opt.k;
+  const int lo = ((k + 1) >> 1) - 1;
+  const int* off = src.st->off;
+  int f0 = 0;
+  for (int r = 0; r < k; r++) {
+    const int c0 = src.cell(min(max(v - lo + r, 0), H - 1), u - lo);
+    const int jb = off[c0], jend = off[c0 + k];
+    int j = jb, c = c0, cell_end = off[c0 + 1], nk = 0;
+    while (j < jend) {
+      while (j >= cell_end) {
+        c++;
+        cell_end = off[c + 1];
+        nk = 0;
+      }
+      if (nk >= cap) {
+        j = cell_end;
+        continue;
+      }
+      if (body(src.fetch(a, j), f0 + (j - jb))) nk++;
+      j++;
+    }
+    f0 += jend - jb;
+  }
+}
+
+// Visit the candidates whose window positions are set in a kept mask (nw
+// words, stride kThreads), in order; the position is mapped back to the stage
+// row by row.
+template <class Body>
+__device__ __forceinline__ void walk_kept(const SampleArgs& a, const SrcStaged& src, int v, int u,
+                                          const unsigned* mask, int nw, Body&& body) {
+  const int H = a.cam.height, k = a.opt.k;
+  const int lo = ((k + 1) >> 1) - 1;
+  const int* off = src.st->off;
+  int r = -1, rf0 = 0, rf1 = 0, jb = 0;
+  for (int w = 0; w < nw; w++) {
+    unsigned m = mask[w * kThreads];
+    while (m) {
+      const int f = (w << 5) + __ffs(m) - 1;
+      m &= m - 1;
+      while (f >= rf1) {
+        r++;
+        const int c0 = src.cell(min(max(v - lo + r, 0), H - 1), u - lo);
+        jb = off[c0];
+        rf0 = rf1;
+        rf1 += off[c0 + k] - jb;
+      }
+      body(src.fetch(a, jb + (f - rf0)));
+    }
+  }
+}
+
 // Fill n elements from p with v using 16-byte stores where aligned.
 template <typename T>
 __device__ __forceinline__ void fill_run(T* p, int n, T v) {
@@ -268,8 +327,12 @@ __device__ __forceinline__ float ray_t(const Ray& r, bool unit, float px, float 
   return unit ? num : __fdiv_rn(num, r.dd);
 }
 
+// `kept` (staged tiles only; else null) is this thread's kept-candidate mask
+// (kMaskWords words, stride kThreads).  For windows with unclamped columns and
+// at most kMaskWords * 32 candidates, pass A records the positions it keeps
+// there and pass B visits only those, without the radius test or the cap.
 template <class Src>
-__device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, int v, int u) {
+__device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, int v, int u, unsigned* kept) {
   const int W = a.cam.width;
   const int ray = v * W + u;
   const int S = a.opt.S, P = a.opt.P;
@@ -280,9 +343,26 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
   const bool unit = r.dd == 1.0f;
   const RadiusTest rt = make_radius_test(radius);
 
+  // the window's candidate count when the kept mask is used, else -1
+  int masked_T = -1;
+  if constexpr (Src::kStaged) {
+    const int k = a.opt.k, lo = ((k + 1) >> 1) - 1, hi = k - 1 - lo;
+    if (kept && u - lo >= 0 && u + hi <= W - 1) {
+      int T = 0;
+      for (int q = 0; q < k; q++) {
+        const int c0 = src.cell(min(max(v - lo + q, 0), a.cam.height - 1), u - lo);
+        T += src.st->off[c0 + k] - src.st->off[c0];
+      }
+      if (T <= kMaskWords * 32) {
+        masked_T = T;
+        for (int w = 0; w < (T + 31) >> 5; w++) kept[w * kThreads] = 0u;
+      }
+    }
+  }
+
   // pass A: tmin / tmax over the kept candidates (epcq_render_topk.cu:132-161)
   float tmin = 1e3f, tmax = -1e3f;
-  walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
+  auto keep = [&](const float4& p) -> bool {
     if (__float_as_int(p.w) < 0) return false;
     float s0, s1, s2;
     const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
@@ -293,7 +373,27 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
     if (tmin > t) tmin = t;
     if (tmax < t) tmax = t;
     return true;
-  });
+  };
+  bool masked = false;
+  if constexpr (Src::kStaged) {
+    if (masked_T >= 0) {
+      masked = true;
+      unsigned word = 0u;
+      int wi = 0;
+      walk_rows(a, src, v, u, kKeptPerCell, [&](const float4& p, int f) -> bool {
+        if (!keep(p)) return false;
+        if ((f >> 5) != wi) {
+          if (word) kept[wi * kThreads] = word;
+          wi = f >> 5;
+          word = 0u;
+        }
+        word |= 1u << (f & 31);
+        return true;
+      });
+      if (word) kept[wi * kThreads] = word;
+    }
+  }
+  if (!masked) walk_window(a, src, v, u, kKeptPerCell, keep);
 
   float* o_xyz = a.sp_xyz + (size_t)ray * S * 3;
   float* o_t = a.sp_t + (size_t)ray * S;
@@ -315,30 +415,25 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
 #pragma unroll
       for (int q = 0; q < kBinList; q++) lb[q] = 0x7fffffff, lc[q] = 0, ls[q] = 0.0f;
       int m = 0, cut = kBins;
-      walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
-        if (__float_as_int(p.w) < 0) return false;
-        float s0, s1, s2;
-        const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
-        const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
-        const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
-        const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
-        if (!within_radius(rt, e0, e1, e2)) return false;
+      // a kept candidate at depth t: into the list if its bin is among the
+      // kBinList smallest in [lo, cut); dist() gives its distance to the ray
+      auto collect = [&](float t, auto&& dist) {
         const int b = bin_index(bdiv, __fsub_rn(t, tmin));
-        if (b < lo || b >= cut) return true;
+        if (b < lo || b >= cut) return;
         if (m == kBinList && b > lb[kBinList - 1]) {
           cut = b;
-          return true;
+          return;
         }
-        const float dist = norm3df(e0, e1, e2);
+        const float d = dist();
         bool found = false;
 #pragma unroll
         for (int q = 0; q < kBinList; q++)
           if (q < m && lb[q] == b) {
             lc[q] += 1;
-            ls[q] = __fadd_rn(ls[q], dist);
+            ls[q] = __fadd_rn(ls[q], d);
             found = true;
           }
-        if (found) return true;
+        if (found) return;
         int pos = 0;
 #pragma unroll
         for (int q = 0; q < kBinList; q++) pos += (q < m && lb[q] < b) ? 1 : 0;
@@ -352,12 +447,38 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
           } else if (q == pos) {
             lb[q] = b;
             lc[q] = 1;
-            ls[q] = dist;
+            ls[q] = d;
           }
         }
         m = m < kBinList ? m + 1 : kBinList;
-        return true;
-      });
+      };
+      bool visited = false;
+      if constexpr (Src::kStaged) {
+        if (masked) {
+          visited = true;
+          walk_kept(a, src, v, u, kept, (masked_T + 31) >> 5, [&](const float4& p) {
+            float s0, s1, s2;
+            const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
+            collect(t, [&] {
+              return norm3df(__fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0])), __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1])),
+                             __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2])));
+            });
+          });
+        }
+      }
+      if (!visited) {
+        walk_window(a, src, v, u, kKeptPerCell, [&](const float4& p) -> bool {
+          if (__float_as_int(p.w) < 0) return false;
+          float s0, s1, s2;
+          const float t = ray_t(r, unit, p.x, p.y, p.z, s0, s1, s2);
+          const float e0 = __fsub_rn(p.x, __fmaf_rn(t, r.d[0], r.o[0]));
+          const float e1 = __fsub_rn(p.y, __fmaf_rn(t, r.d[1], r.o[1]));
+          const float e2 = __fsub_rn(p.z, __fmaf_rn(t, r.d[2], r.o[2]));
+          if (!within_radius(rt, e0, e1, e2)) return false;
+          collect(t, [&] { return norm3df(e0, e1, e2); });
+          return true;
+        });
+      }
       // primary-surface walk (epcq_render_topk.cu:181-204)
       bool done = false;
 #pragma unroll
@@ -1033,9 +1154,9 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
       if (rk < nvalid) {
         const int px = st.order[rk];
         if (staged)
-          sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
+          sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31), &st.kept[0][tid]);
         else
-          sample_ray(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
+          sample_ray(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31), nullptr);
       }
       continue;
     }
