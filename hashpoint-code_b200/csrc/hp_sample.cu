@@ -44,6 +44,7 @@
 // adds them with shared-memory atomics in an unspecified order, so a bin's
 // mean distance can differ from the reference's in the last bit -- which moves
 // an output only if alpha * T or T sits within that bit of 1e-3.
+#include <cstdio>
 #include <mutex>
 
 #include "hp_common.cuh"
@@ -63,13 +64,10 @@ constexpr int kSplitWork = kStageCap;  // tiles whose halo holds more points are
 constexpr int kBinList = HP_BIN_LIST;  // distinct t-bins collected per candidate pass
 constexpr int kTeReg = 4;        // emitted sample depths kept in registers
 constexpr int kBallPass = 2;     // samples served by one ball-query walk
-#ifndef HP_HEAVY_WINDOW
-#define HP_HEAVY_WINDOW 320
-#endif
-constexpr int kHeavyWindow = HP_HEAVY_WINDOW;  // rays with more window candidates get a whole warp
-constexpr int kMaskWords = (kHeavyWindow + 31) / 32;  // kept-candidate mask of a thread-served ray
+constexpr int kHeavyWindow = 320;  // default: rays with more window candidates get a whole warp
+constexpr int kMaxHeavyWindow = 320;  // largest window a thread serves (its kept mask's size)
+constexpr int kMaskWords = (kMaxHeavyWindow + 31) / 32;  // kept-candidate mask of a thread-served ray
 constexpr int kClasses = 64;     // window-size classes used to group a tile's rays
-constexpr int kClassWidth = kHeavyWindow / 40 > 0 ? kHeavyWindow / 40 : 1;  // candidates per class
 constexpr int kWalkBatch = 4;    // bins whose sums one walk pass of a warp-served ray gathers
 
 struct SampleArgs {
@@ -84,6 +82,7 @@ struct SampleArgs {
   int* __restrict__ pc_idx;
   float* __restrict__ sp_t;
   uint8_t* __restrict__ mask;
+  int heavy;  // rays with more window candidates than this are served by a whole warp (<= kMaxHeavyWindow)
 };
 
 struct Stage {
@@ -951,6 +950,7 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
 struct Sched {
   int* work;    // [max items] estimated cost
   int* item;    // [max items] (tile << 8) | (first row << 4) | rows
+  int* view;    // [max items] view of the item (batched launches; else null)
   int* order;   // [max items] item indices, heaviest first
   int* counts;  // [32] items per cost class
   int* fill;    // [32] placement cursors
@@ -977,11 +977,10 @@ __device__ __forceinline__ int halo_points(const int2* __restrict__ hash, int n_
   return sum;
 }
 
-__global__ void __launch_bounds__(256) k_tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k,
-                                                   int tiles_x, int ntiles, Sched sc) {
+// Items of tile t (local to its view) of an H x W image, appended to the queue.
+__device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k, int tiles_x,
+                                          int t, int view, Sched& sc) {
   const int lane = threadIdx.x & 31;
-  const int t = blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (t >= ntiles) return;
   const int v0 = (t / tiles_x) * kTileH, u0 = (t % tiles_x) * kTileW;
   const int v_end = min(H, v0 + kTileH);
   // split the tile's rows until each item's halo holds at most kSplitWork
@@ -1001,10 +1000,18 @@ __global__ void __launch_bounds__(256) k_tile_work(const int2* __restrict__ hash
       const int i = atomicAdd(sc.n_items, 1);
       sc.work[i] = w;
       sc.item[i] = (t << 8) | ((vb - v0) << 4) | rows;
+      if (sc.view) sc.view[i] = view;
       atomicAdd(sc.counts + cost_class(w), 1);
     }
     vb += rows;
   }
+}
+
+__global__ void __launch_bounds__(256) k_tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k,
+                                                   int tiles_x, int ntiles, Sched sc) {
+  const int t = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (t >= ntiles) return;
+  tile_work(hash, n_sorted, H, W, k, tiles_x, t, 0, sc);
 }
 
 __global__ void __launch_bounds__(256) k_tile_order(Sched sc) {
@@ -1093,7 +1100,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
   // Group the tile's rays by their window's candidate count (a counting sort
   // over size classes; the order within a class does not affect any output).
   // The warps then pull work units, longest first: groups of 32 consecutive ranks below
-  // kHeavyWindow candidates (one ray per thread, similar loop lengths; a group
+  // a.heavy candidates (one ray per thread, similar loop lengths; a group
   // runs as long as its heaviest ray), then one unit per heavier ray (served by
   // the whole warp, sample_ray_warp, in about a 32nd of that time).  Warps that
   // finish early take the next unit, so a tile ends within about one short
@@ -1123,8 +1130,8 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
     if (tid == 0) st.next_unit = 0;
     __syncthreads();
     // class 0: warp-served rays; then light rays by descending window size; last: no ray
-    const int c = T < 0 ? kClasses - 1
-                        : (T > kHeavyWindow ? 0 : 1 + min(kClasses - 3, (kHeavyWindow - T) / kClassWidth));
+    const int cw = max(1, a.heavy / 40);  // candidates per class
+    const int c = T < 0 ? kClasses - 1 : (T > a.heavy ? 0 : 1 + min(kClasses - 3, (a.heavy - T) / cw));
     const int local = atomicAdd(&st.cls[c], 1);
     __syncthreads();
     if (tid < 32) {
@@ -1187,6 +1194,106 @@ __global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a, Sc
   }
 }
 
+// ---------------------------------------------------------------------------
+// Batched launch: the tiles of many views (different clouds, cameras, image
+// sizes and options) in one queue and one persistent sampling kernel, so a
+// view's tail overlaps the other views' work.  Every ray runs the same code as
+// in a per-view launch, so the outputs are identical.
+
+// Device view table -> per-view kernel arguments and the first global tile of
+// each view (exclusive scan; tile_base[n_views] = all tiles).  One warp.
+__global__ void k_batch_setup(const hp_view* __restrict__ views, int n_views, int heavy,
+                              SampleArgs* __restrict__ args, int* __restrict__ tile_base) {
+  const int lane = threadIdx.x;
+  int run = 0;
+  for (int b = 0; b < n_views; b += 32) {
+    const int v = b + lane;
+    int tiles = 0;
+    if (v < n_views) {
+      const hp_view& hv = views[v];
+      SampleArgs a;
+      a.xyz = hv.xyz;
+      a.sidx = hv.sorted_point_idx;
+      a.hash = (const int2*)hv.hash_table;
+      a.n_points = (int)hv.n_points;
+      a.n_sorted = (int)hv.n_sorted;
+      a.cam.c2w = hv.cam.c2w;
+      a.cam.fx = hv.cam.fx;
+      a.cam.fy = hv.cam.fy;
+      a.cam.cx = hv.cam.cx;
+      a.cam.cy = hv.cam.cy;
+      a.cam.width = hv.cam.width;
+      a.cam.height = hv.cam.height;
+      a.opt.k = hv.opt.kernel_size;
+      a.opt.t_intvl = hv.opt.t_intvl;
+      a.opt.radius = hv.opt.radius_threshold;
+      a.opt.S = hv.opt.num_sample_points_per_ray;
+      a.opt.P = hv.opt.num_point_cloud_per_sp;
+      a.opt.num_point_per_ray = hv.opt.num_point_per_ray;
+      a.opt.alpha_g = hv.opt.sdf2weight_gaussian_alpha;
+      a.opt.gamma = hv.opt.sdf2weight_gaussian_gamma;
+      a.sp_xyz = hv.sp_xyz;
+      a.pc_idx = hv.pc_idx;
+      a.sp_t = hv.sp_t;
+      a.mask = hv.mask;
+      a.heavy = heavy;
+      args[v] = a;
+      tiles = ((hv.cam.width + kTileW - 1) / kTileW) * ((hv.cam.height + kTileH - 1) / kTileH);
+    }
+    int incl = tiles;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (v < n_views) tile_base[v] = run + incl - tiles;
+    run += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  if (lane == 0) tile_base[n_views] = run;
+}
+
+// One warp per global tile: find its view, then queue the tile's items.
+__global__ void __launch_bounds__(256) k_batch_tile_work(const SampleArgs* __restrict__ args,
+                                                         const int* __restrict__ tile_base, int n_views,
+                                                         int total_tiles, Sched sc) {
+  const int g = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (g >= total_tiles) return;
+  int lo = 0, hi = n_views;  // tile_base[lo] <= g < tile_base[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (tile_base[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const SampleArgs& a = args[lo];
+  const int tiles_x = (a.cam.width + kTileW - 1) / kTileW;
+  tile_work(a.hash, a.n_sorted, a.cam.height, a.cam.width, a.opt.k, tiles_x, g - tile_base[lo], lo, sc);
+}
+
+// The persistent sampling kernel over the batch's queue; each item's view
+// arguments are loaded into shared memory before the tile is processed.
+__global__ void __launch_bounds__(kThreads, 3) k_quick_sampling_batch(const SampleArgs* __restrict__ args, Sched sc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Stage& st = *reinterpret_cast<Stage*>(smem_raw);
+  __shared__ int s_next;
+  __shared__ SampleArgs s_args;
+  const int n = *sc.n_items;
+  for (;;) {
+    if (threadIdx.x == 0) s_next = atomicAdd(sc.next, 1);
+    __syncthreads();
+    const int i = s_next;
+    if (i >= n) break;
+    const int j = sc.order[i];
+    if (threadIdx.x == 0) s_args = args[sc.view[j]];
+    __syncthreads();
+    const int it = sc.item[j];
+    const int t = it >> 8;
+    const int tiles_x = (s_args.cam.width + kTileW - 1) / kTileW;
+    process_tile(s_args, st, (t / tiles_x) * kTileH + ((it >> 4) & 15), it & 15, (t % tiles_x) * kTileW);
+  }
+}
+
 __global__ void k_ray_directions(DevCamera cam, float* __restrict__ dirs) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= cam.width * cam.height) return;
@@ -1199,9 +1306,9 @@ __global__ void k_ray_directions(DevCamera cam, float* __restrict__ dirs) {
 
 // The stage exceeds the 48 KB default of dynamic shared memory: opt the kernel
 // in once per device and size the persistent grid from its occupancy.
-int32_t sampling_grid(int* blocks) {
+int32_t sampling_grid(int* blocks, int* sm_count = nullptr) {
   static std::mutex mu;
-  static int grid[128] = {0};
+  static int grid[128] = {0}, sm_counts[128] = {0};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
     return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaGetDevice failed");
@@ -1209,21 +1316,25 @@ int32_t sampling_grid(int* blocks) {
   if (!grid[dev]) {
     cudaError_t e =
         cudaFuncSetAttribute(k_quick_sampling, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Stage));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_quick_sampling_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Stage));
     int sms = 0, per_sm = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_quick_sampling, kThreads, sizeof(Stage));
     if (e != cudaSuccess) return set_error(HP_ERR_CUDA, "hp_quick_sampling: kernel set-up: %s", cudaGetErrorString(e));
     grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
+    sm_counts[dev] = sms;
   }
   *blocks = grid[dev];
+  if (sm_count) *sm_count = sm_counts[dev];
   return HP_OK;
 }
 
 static constexpr size_t align256s(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct SchedLayout {
-  size_t work, item, order, small, total;
+  size_t work, item, order, view, small, total;
 };
 
 // up to kTileH items per tile (every row its own item)
@@ -1234,9 +1345,33 @@ static SchedLayout sched_layout(int64_t H, int64_t W) {
   L.work = 0;
   L.item = per;
   L.order = 2 * per;
+  L.view = 0;  // single view: none
   L.small = 3 * per;
   L.total = L.small + 512;  // counts[32], fill[32], next, n_items
   return L;
+}
+
+// Batched launch: the queue over all views' tiles, then the per-view
+// arguments, the views' first tiles and room for a copy of the view table.
+struct BatchLayout {
+  SchedLayout q;
+  size_t args, tile_base, views, total;
+};
+
+static BatchLayout batch_layout(int64_t total_tiles, int n_views) {
+  BatchLayout B;
+  const size_t per = align256s(sizeof(int) * (size_t)(total_tiles * kTileH));
+  B.q.work = 0;
+  B.q.item = per;
+  B.q.order = 2 * per;
+  B.q.view = 3 * per;
+  B.q.small = 4 * per;
+  B.q.total = B.q.small + 512;
+  B.args = B.q.total;
+  B.tile_base = B.args + align256s(sizeof(SampleArgs) * (size_t)n_views);
+  B.views = B.tile_base + align256s(sizeof(int) * (size_t)(n_views + 1));
+  B.total = B.views + align256s(sizeof(hp_view) * (size_t)n_views);
+  return B;
 }
 
 int32_t check_camera(const hp_camera* cam, const char* who) {
@@ -1281,32 +1416,41 @@ extern "C" size_t hp_quick_sampling_workspace_size(int32_t height, int32_t width
   return sched_layout(height, width).total;
 }
 
+// Argument checks shared by the per-view and batched entry points.
+static int32_t check_sampling(const char* who, const float* xyz, int64_t n_points, const hp_camera* cam,
+                              const hp_options* opt, const int32_t* sorted_point_idx, int64_t n_sorted,
+                              const int32_t* hash_table, const float* sp_xyz, const int32_t* pc_idx, const float* sp_t,
+                              const uint8_t* mask) {
+  if (int32_t rc = check_camera(cam, who)) return rc;
+  if (!opt) return set_error(HP_ERR_INVALID_ARGUMENT, "%s: opt is NULL", who);
+  if (opt->kernel_size < 1 || opt->kernel_size > kMaxKernel)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "%s: kernel_size %d outside 1..%d (the reference's windows hold 32 cells)",
+                     who, opt->kernel_size, kMaxKernel);
+  if (!(opt->t_intvl > 0.0f)) return set_error(HP_ERR_INVALID_ARGUMENT, "%s: t_intvl must be > 0", who);
+  if (opt->num_sample_points_per_ray < 1 || opt->num_point_cloud_per_sp < 1)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "%s: num_sample_points_per_ray and num_point_cloud_per_sp must be >= 1",
+                     who);
+  const int64_t hw = (int64_t)cam->height * cam->width;
+  if (hw * opt->num_sample_points_per_ray * (int64_t)(opt->num_point_cloud_per_sp > 3 ? opt->num_point_cloud_per_sp : 3) >=
+      (1ll << 40))
+    return set_error(HP_ERR_INVALID_ARGUMENT, "%s: output too large", who);
+  if (n_points < 0 || n_points >= (1ll << 31) || n_sorted < 0 || n_sorted >= (1ll << 31))
+    return set_error(HP_ERR_INVALID_ARGUMENT, "%s: n_points / n_sorted out of range", who);
+  if (!hash_table || !sp_xyz || !pc_idx || !sp_t || !mask || (n_points > 0 && !xyz) ||
+      (n_sorted > 0 && !sorted_point_idx))
+    return set_error(HP_ERR_INVALID_ARGUMENT, "%s: null pointer", who);
+  if (((uintptr_t)hash_table & 7) != 0)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "%s: hash_table must be 8-byte aligned", who);
+  return HP_OK;
+}
+
 extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const hp_camera* cam, const hp_options* opt,
                                      const int32_t* sorted_point_idx, int64_t n_sorted, const int32_t* hash_table,
                                      float* sp_xyz, int32_t* pc_idx, float* sp_t, uint8_t* mask, void* workspace,
                                      size_t workspace_bytes, hp_stream_t stream) {
-  if (int32_t rc = check_camera(cam, "hp_quick_sampling")) return rc;
-  if (!opt) return set_error(HP_ERR_INVALID_ARGUMENT, "hp_quick_sampling: opt is NULL");
-  if (opt->kernel_size < 1 || opt->kernel_size > kMaxKernel)
-    return set_error(HP_ERR_INVALID_ARGUMENT,
-                     "hp_quick_sampling: kernel_size %d outside 1..%d (the reference's windows hold 32 cells)",
-                     opt->kernel_size, kMaxKernel);
-  if (!(opt->t_intvl > 0.0f))
-    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_quick_sampling: t_intvl must be > 0");
-  if (opt->num_sample_points_per_ray < 1 || opt->num_point_cloud_per_sp < 1)
-    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_quick_sampling: num_sample_points_per_ray and "
-                     "num_point_cloud_per_sp must be >= 1");
-  const int64_t hw = (int64_t)cam->height * cam->width;
-  if (hw * opt->num_sample_points_per_ray * (int64_t)(opt->num_point_cloud_per_sp > 3 ? opt->num_point_cloud_per_sp : 3) >=
-      (1ll << 40))
-    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_quick_sampling: output too large");
-  if (n_points < 0 || n_points >= (1ll << 31) || n_sorted < 0 || n_sorted >= (1ll << 31))
-    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_quick_sampling: n_points / n_sorted out of range");
-  if (!hash_table || !sp_xyz || !pc_idx || !sp_t || !mask || (n_points > 0 && !xyz) ||
-      (n_sorted > 0 && !sorted_point_idx))
-    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_quick_sampling: null pointer");
-  if (((uintptr_t)hash_table & 7) != 0)
-    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_quick_sampling: hash_table must be 8-byte aligned");
+  if (int32_t rc = check_sampling("hp_quick_sampling", xyz, n_points, cam, opt, sorted_point_idx, n_sorted, hash_table,
+                                  sp_xyz, pc_idx, sp_t, mask))
+    return rc;
   const SchedLayout L = sched_layout(cam->height, cam->width);
   if (!workspace || workspace_bytes < L.total || ((uintptr_t)workspace & 255) != 0)
     return set_error(HP_ERR_WORKSPACE, "hp_quick_sampling: workspace needs %zu bytes, 256-byte aligned (got %zu)",
@@ -1323,6 +1467,7 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   a.pc_idx = pc_idx;
   a.sp_t = sp_t;
   a.mask = mask;
+  a.heavy = kHeavyWindow;
   int blocks = 0;
   if (int32_t rc = sampling_grid(&blocks)) return rc;
   const int tiles_x = (cam->width + kTileW - 1) / kTileW;
@@ -1332,6 +1477,7 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   sc.work = (int*)(ws + L.work);
   sc.item = (int*)(ws + L.item);
   sc.order = (int*)(ws + L.order);
+  sc.view = nullptr;
   sc.counts = (int*)(ws + L.small);
   sc.fill = sc.counts + 32;
   sc.next = sc.counts + 64;
@@ -1346,6 +1492,82 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   if (int32_t rc = check_launch("k_tile_order")) return rc;
   k_quick_sampling<<<blocks < ntiles ? blocks : ntiles, kThreads, sizeof(Stage), st>>>(a, sc, tiles_x);
   return check_launch("k_quick_sampling");
+}
+
+static int64_t batch_tiles(const hp_view* views, int32_t n_views) {
+  int64_t total = 0;
+  for (int32_t v = 0; v < n_views; v++)
+    total += (int64_t)((views[v].cam.width + kTileW - 1) / kTileW) * ((views[v].cam.height + kTileH - 1) / kTileH);
+  return total;
+}
+
+extern "C" size_t hp_quick_sampling_batch_workspace_size(const hp_view* views, int32_t n_views) {
+  if (!views || n_views <= 0) return 0;
+  for (int32_t v = 0; v < n_views; v++)
+    if (views[v].cam.width <= 0 || views[v].cam.height <= 0) return 0;
+  return batch_layout(batch_tiles(views, n_views), n_views).total;
+}
+
+extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* views_device, int32_t n_views,
+                                           const hp_tuning* tuning, void* workspace, size_t workspace_bytes,
+                                           hp_stream_t stream) {
+  static const char* who = "hp_quick_sampling_batch";
+  if (!views || n_views <= 0) return set_error(HP_ERR_INVALID_ARGUMENT, "%s: no views", who);
+  int heavy = kHeavyWindow, per_sm = 0;
+  if (tuning) {
+    if (tuning->heavy_window < 0 || tuning->heavy_window > kMaxHeavyWindow || tuning->blocks_per_sm < 0)
+      return set_error(HP_ERR_INVALID_ARGUMENT, "%s: tuning out of range (heavy_window 0..%d, blocks_per_sm >= 0)",
+                       who, kMaxHeavyWindow);
+    if (tuning->heavy_window > 0) heavy = tuning->heavy_window;
+    per_sm = tuning->blocks_per_sm;
+  }
+  for (int32_t v = 0; v < n_views; v++) {
+    const hp_view& hv = views[v];
+    if (int32_t rc = check_sampling(who, hv.xyz, hv.n_points, &hv.cam, &hv.opt, hv.sorted_point_idx, hv.n_sorted,
+                                    hv.hash_table, hv.sp_xyz, hv.pc_idx, hv.sp_t, hv.mask)) {
+      char msg[256];
+      snprintf(msg, sizeof(msg), "%s", hp_last_error());
+      return set_error(rc, "%s (view %d)", msg, v);
+    }
+  }
+  const int64_t total_tiles = batch_tiles(views, n_views);
+  if (total_tiles * kTileH >= (1ll << 31)) return set_error(HP_ERR_INVALID_ARGUMENT, "%s: too many tiles", who);
+  const BatchLayout B = batch_layout(total_tiles, n_views);
+  if (!workspace || workspace_bytes < B.total || ((uintptr_t)workspace & 255) != 0)
+    return set_error(HP_ERR_WORKSPACE, "%s: workspace needs %zu bytes, 256-byte aligned (got %zu)", who, B.total,
+                     workspace_bytes);
+  int blocks = 0, sms = 0;
+  if (int32_t rc = sampling_grid(&blocks, &sms)) return rc;
+  if (per_sm > 0 && per_sm * sms < blocks) blocks = per_sm * sms;
+  char* ws = (char*)workspace;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!views_device) {  // copy the table into the workspace
+    if (cudaMemcpyAsync(ws + B.views, views, sizeof(hp_view) * (size_t)n_views, cudaMemcpyHostToDevice, st) !=
+        cudaSuccess)
+      return set_error(HP_ERR_CUDA, "%s: copying the view table failed", who);
+    views_device = (const hp_view*)(ws + B.views);
+  }
+  Sched sc;
+  sc.work = (int*)(ws + B.q.work);
+  sc.item = (int*)(ws + B.q.item);
+  sc.order = (int*)(ws + B.q.order);
+  sc.view = (int*)(ws + B.q.view);
+  sc.counts = (int*)(ws + B.q.small);
+  sc.fill = sc.counts + 32;
+  sc.next = sc.counts + 64;
+  sc.n_items = sc.counts + 65;
+  SampleArgs* args = (SampleArgs*)(ws + B.args);
+  int* tile_base = (int*)(ws + B.tile_base);
+  if (cudaMemsetAsync(sc.counts, 0, 512, st) != cudaSuccess) return set_error(HP_ERR_CUDA, "%s: memset failed", who);
+  k_batch_setup<<<1, 32, 0, st>>>(views_device, n_views, heavy, args, tile_base);
+  if (int32_t rc = check_launch("k_batch_setup")) return rc;
+  const int nt = (int)total_tiles;
+  k_batch_tile_work<<<(nt + 7) / 8, 256, 0, st>>>(args, tile_base, n_views, nt, sc);
+  if (int32_t rc = check_launch("k_batch_tile_work")) return rc;
+  k_tile_order<<<(nt + 255) / 256 < 148 ? (nt + 255) / 256 : 148, 256, 0, st>>>(sc);
+  if (int32_t rc = check_launch("k_tile_order")) return rc;
+  k_quick_sampling_batch<<<blocks < nt ? blocks : nt, kThreads, sizeof(Stage), st>>>(args, sc);
+  return check_launch("k_quick_sampling_batch");
 }
 
 extern "C" int32_t hp_ray_directions(const hp_camera* cam, float* dirs, hp_stream_t stream) {

@@ -30,8 +30,9 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
 
 # C-ABI symbols declared in include/hashpoint_b200.h
 EXPORTS = ["hp_version", "hp_last_error", "hp_projection_rounding", "hp_pts2plane_workspace_size", "hp_pts2plane",
-           "hp_pts2plane_noalloc", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling", "hp_quick_query_for_nearby_point", "hp_scatter",
-           "hp_ray_directions"]
+           "hp_pts2plane_noalloc", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling",
+           "hp_quick_sampling_batch_workspace_size", "hp_quick_sampling_batch", "hp_quick_query_for_nearby_point",
+           "hp_scatter", "hp_ray_directions"]
 
 HP_OK = 0
 
@@ -103,6 +104,19 @@ class HpOptions(ctypes.Structure):
                 ("sdf2weight_gaussian_alpha", ctypes.c_float), ("sdf2weight_gaussian_gamma", ctypes.c_float)]
 
 
+class HpTuning(ctypes.Structure):
+    """Launch tuning of hp_quick_sampling_batch (0 = default)."""
+    _fields_ = [("heavy_window", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32)]
+
+
+class HpView(ctypes.Structure):
+    """One view of hp_quick_sampling_batch (include/hashpoint_b200.h)."""
+    _fields_ = [("xyz", ctypes.c_void_p), ("n_points", ctypes.c_int64), ("sorted_point_idx", ctypes.c_void_p),
+                ("n_sorted", ctypes.c_int64), ("hash_table", ctypes.c_void_p), ("sp_xyz", ctypes.c_void_p),
+                ("pc_idx", ctypes.c_void_p), ("sp_t", ctypes.c_void_p), ("mask", ctypes.c_void_p),
+                ("cam", HpCamera), ("opt", HpOptions)]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -137,6 +151,11 @@ def lib():
         L.hp_quick_sampling_workspace_size.restype = sz
         L.hp_quick_sampling.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, vp, vp, vp, vp, sz, vp]
         L.hp_quick_sampling.restype = i32
+        view_p = ctypes.POINTER(HpView)
+        L.hp_quick_sampling_batch_workspace_size.argtypes = [view_p, i32]
+        L.hp_quick_sampling_batch_workspace_size.restype = sz
+        L.hp_quick_sampling_batch.argtypes = [view_p, vp, i32, ctypes.POINTER(HpTuning), vp, sz, vp]
+        L.hp_quick_sampling_batch.restype = i32
         L.hp_quick_query_for_nearby_point.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, i64, vp, vp]
         L.hp_quick_query_for_nearby_point.restype = i32
         L.hp_scatter.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp]

@@ -144,6 +144,60 @@ def quick_sampling(xyz, c2w, fx, fy, cx, cy, width, height, opt, sorted_point_id
     return sp_xyz, pc_idx, sp_t, mask
 
 
+def sampling_outputs(height, width, opt, device):
+    """Uninitialised quick_sampling outputs (every element is written by the kernel)."""
+    H, W = int(height), int(width)
+    S, P = int(opt.num_sample_points_per_ray), int(opt.num_point_cloud_per_sp)
+    return (torch.empty((H, W, S, 3), dtype=torch.float32, device=device),
+            torch.empty((H, W, S, P), dtype=torch.int32, device=device),
+            torch.empty((H, W, S), dtype=torch.float32, device=device),
+            torch.empty((H, W, S), dtype=torch.bool, device=device))
+
+
+def make_view(xyz, c2w, fx, fy, cx, cy, width, height, opt, sorted_point_idx, hash_table, outputs):
+    """HpView for hp_quick_sampling_batch (the caller keeps the tensors alive)."""
+    check_input(xyz, "xyz_data", torch.float32)
+    check_matrix(c2w, "c2w")
+    check_input(sorted_point_idx, "sorted_point_idx_list", torch.int32)
+    H, W = int(height), int(width)
+    hash_table = _hash_view(hash_table, H, W)
+    sp_xyz, pc_idx, sp_t, mask = outputs
+    v = native.HpView()
+    v.xyz, v.n_points = _ptr(xyz).value, xyz.shape[0]
+    v.sorted_point_idx, v.n_sorted = _ptr(sorted_point_idx).value, sorted_point_idx.numel()
+    v.hash_table = _ptr(hash_table).value
+    v.sp_xyz, v.pc_idx, v.sp_t, v.mask = (_ptr(sp_xyz).value, _ptr(pc_idx).value, _ptr(sp_t).value,
+                                          _ptr(mask).value)
+    v.cam = make_camera(c2w=c2w, fx=fx, fy=fy, cx=cx, cy=cy, width=W, height=H)
+    v.opt = make_options(opt)
+    return v
+
+
+def batch_workspace_size(views):
+    n = len(views)
+    return native.lib().hp_quick_sampling_batch_workspace_size((native.HpView * n)(*views), n)
+
+
+def quick_sampling_batch(views, device, views_device=None, workspace=None, heavy_window=0, blocks_per_sm=0):
+    """hp_quick_sampling_batch over a list of HpView (see make_view); outputs are the views' own tensors.
+
+    views_device: optional uint8 CUDA tensor holding the same table (for CUDA-graph capture).
+    workspace: optional uint8 CUDA tensor of at least batch_workspace_size(views) bytes.
+    heavy_window, blocks_per_sm: launch tuning (0 = default); outputs do not depend on it."""
+    L = native.lib()
+    n = len(views)
+    table = (native.HpView * n)(*views)
+    ws_bytes = L.hp_quick_sampling_batch_workspace_size(table, n)
+    if ws_bytes == 0:
+        raise RuntimeError("hp_quick_sampling_batch: invalid views")
+    if workspace is None:
+        workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=device)
+    tuning = native.HpTuning(int(heavy_window), int(blocks_per_sm))
+    rc = L.hp_quick_sampling_batch(table, _ptr(views_device), n, ctypes.byref(tuning), _ptr(workspace),
+                                   workspace.numel(), _stream(torch.device(device)))
+    native.check(rc, "hp_quick_sampling_batch")
+
+
 def quick_query(xyz, c2w, fx, fy, cx, cy, width, height, opt, sorted_point_idx, hash_table, ray_ids):
     check_input(xyz, "xyz_data", torch.float32)
     check_matrix(c2w, "c2w")

@@ -273,3 +273,33 @@ def check_in_front(xyz, cam):
     """True when every point has positive camera depth (no behind-camera aliasing)."""
     z = xyz.astype(np.float64) @ cam.w2c[2, :3].astype(np.float64) + float(cam.w2c[2, 3])
     return bool(np.all(z > 0))
+
+
+@dataclass
+class MixedBatch:
+    """Several clouds and views over them (view = (cloud index, camera))."""
+    clouds: list
+    views: list
+    options: Options
+
+
+MIXED_RESOLUTIONS = ((256, 256), (512, 512), (800, 800), (1600, 1200))
+
+
+def make_mixed(n_clouds=8, n_views=64, seed=0, size_range=(5e4, 4e6), resolutions=MIXED_RESOLUTIONS):
+    """Uneven multi-cloud batch: clouds as in `shapes` with sizes log-uniform in
+    size_range; each view picks a cloud and a resolution uniformly, f = 1111 * W / 800,
+    camera on the radius-4 sphere looking at the origin."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(size_range[0]), np.log(size_range[1])
+    sizes = np.exp(rng.uniform(lo, hi, size=n_clouds)).astype(np.int64)
+    clouds = [shapes_cloud(rng, int(n)) for n in sizes]
+    views = []
+    for _ in range(n_views):
+        c = int(rng.integers(n_clouds))
+        W, H = resolutions[int(rng.integers(len(resolutions)))]
+        f = 1111.0 * W / 800.0
+        cam = orbit_cameras(rng, 1, 4.0, W, H, f, W / 2, H / 2)[0]
+        views.append((c, cam))
+    opt = Options(kernel_size=5, radius_threshold=0.008, num_sample_points_per_ray=8, num_point_cloud_per_sp=8)
+    return MixedBatch(clouds, views, opt)

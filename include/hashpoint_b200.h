@@ -146,6 +146,50 @@ HP_API int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const hp_ca
  * schedule); workspace must be 256-byte aligned. */
 HP_API size_t hp_quick_sampling_workspace_size(int32_t height, int32_t width);
 
+/* Launch tuning of hp_quick_sampling_batch (NULL or 0 fields = defaults).
+ * Outputs never depend on it.  heavy_window: rays whose window holds more
+ * candidates are served by a whole warp instead of one thread (0..320;
+ * default 320).  blocks_per_sm: resident blocks of the persistent sampling
+ * kernel per SM (default: as many as fit). */
+typedef struct hp_tuning {
+  int32_t heavy_window;
+  int32_t blocks_per_sm;
+} hp_tuning;
+
+/* One view of a batched hp_quick_sampling: the arguments of hp_quick_sampling
+ * for that view (cloud, camera, options, its hash table and its outputs). */
+typedef struct hp_view {
+  const float* xyz;
+  int64_t n_points;
+  const int32_t* sorted_point_idx;
+  int64_t n_sorted;
+  const int32_t* hash_table;
+  float* sp_xyz;
+  int32_t* pc_idx;
+  float* sp_t;
+  uint8_t* mask;
+  hp_camera cam;
+  hp_options opt;
+} hp_view;
+
+/* hp_quick_sampling for many views -- different clouds, cameras, image sizes
+ * and options -- in one persistent launch over the tiles of all views
+ * (heaviest first), so one view's tail overlaps the other views' work.  Each
+ * view's outputs are bit-identical to hp_quick_sampling's for that view.  No
+ * counterpart call in the reference, which launches quick_sampling once per
+ * view (epcq/csrc/epcq_render_topk.cu:341-417).  `views` (host) is checked and
+ * sizes the launch; the kernels read `views_device`, the same table in device
+ * memory (for example copied there from pinned memory, so the call can be
+ * captured in a CUDA graph), or, when it is NULL, a copy of `views` made into
+ * the workspace on `stream`.  `tuning` may be NULL. */
+HP_API int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* views_device, int32_t n_views,
+                                       const hp_tuning* tuning, void* workspace, size_t workspace_bytes,
+                                       hp_stream_t stream);
+
+/* Scratch bytes hp_quick_sampling_batch needs for these views (0 if invalid);
+ * 256-byte aligned. */
+HP_API size_t hp_quick_sampling_batch_workspace_size(const hp_view* views, int32_t n_views);
+
 /* Ray query for a list of pixel rays (linear ids v*W+u).  Replaces
  * _C.quick_query_for_nearby_point (epcq/csrc/epcq_render_topk.cu:287-339,
  * kernel :222-283).  out [n_rays, num_point_per_ray]: ids with ray distance

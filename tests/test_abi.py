@@ -118,6 +118,35 @@ def test_quick_sampling_rejects_null_and_misaligned(L):
                                None) == -2
 
 
+def _view(w=8, h=8, k=3):
+    v = native.HpView()
+    p = 0x1000
+    v.xyz, v.n_points, v.sorted_point_idx, v.n_sorted, v.hash_table = p, 10, p, 10, p
+    v.sp_xyz = v.pc_idx = v.sp_t = v.mask = p
+    v.cam = _cam(w, h)
+    v.opt = _opt(k)
+    return v
+
+
+def test_batch_workspace_and_validation(L):
+    one = (native.HpView * 1)(_view())
+    two = (native.HpView * 2)(_view(), _view(64, 48))
+    a = L.hp_quick_sampling_batch_workspace_size(one, 1)
+    b = L.hp_quick_sampling_batch_workspace_size(two, 2)
+    assert 0 < a < b
+    assert L.hp_quick_sampling_batch_workspace_size(two, 0) == 0
+    assert L.hp_quick_sampling_batch_workspace_size((native.HpView * 1)(_view(w=0)), 1) == 0
+    ws = ctypes.c_void_p(0x100000)
+    t = native.HpTuning(0, 0)
+    bad = (native.HpView * 2)(_view(), _view(k=9))
+    assert L.hp_quick_sampling_batch(bad, None, 2, ctypes.byref(t), ws, 1 << 30, None) == -1
+    assert "view 1" in _err(L) and "kernel_size" in _err(L)
+    assert L.hp_quick_sampling_batch(two, None, 0, ctypes.byref(t), ws, 1 << 30, None) == -1
+    assert L.hp_quick_sampling_batch(two, None, 2, ctypes.byref(t), ws, b - 1, None) == -2
+    assert L.hp_quick_sampling_batch(two, None, 2, ctypes.byref(native.HpTuning(321, 0)), ws, b, None) == -1
+    assert "tuning" in _err(L)
+
+
 def test_pts2plane_checks_workspace(L):
     p = ctypes.c_void_p(0x1000)
     need = L.hp_pts2plane_workspace_size(10, 8, 8)

@@ -1,0 +1,122 @@
+"""Batched search+sample (hp_quick_sampling_batch, hashpoint.batch) against the
+per-view launch and the reference's golden outputs.
+
+Every view of a batch must come out bit-identical to the same view launched
+alone: the golden fixtures (reference CUDA outputs, mixed options and sizes)
+as one batch, a mixed multi-cloud batch against per-view launches, the device
+view table and a CUDA graph replay, and every launch tuning.
+"""
+import numpy as np
+import pytest
+import torch
+
+from hashpoint import batch, native, ops, synth
+from hp_testutil import Golden, bits, golden_names
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _setup():
+    native.build()
+
+
+def D(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def H(t):
+    return t.cpu().numpy()
+
+
+def _same(a, b):
+    """Bit-identical quick_sampling outputs."""
+    for x, y in zip(a, b):
+        x, y = H(x), H(y)
+        if x.dtype == np.float32:
+            assert np.array_equal(bits(x), bits(y))
+        else:
+            assert np.array_equal(x, y)
+
+
+def test_golden_views_as_one_batch():
+    keep, views, outs = [], [], []
+    for name in golden_names():
+        g = Golden(name)
+        t = dict(xyz=D(g["xyz"]), c2w=D(g["c2w"]), sidx=D(g["sorted_point_idx"]), hash=D(g["hash_table"]))
+        out = ops.sampling_outputs(g.H, g.W, g.opt, "cuda")
+        views.append(ops.make_view(t["xyz"], t["c2w"], g.fx, g.fy, g.cx, g.cy, g.W, g.H, g.opt, t["sidx"], t["hash"],
+                                   out))
+        keep.append((t, g))
+        outs.append(out)
+    ops.quick_sampling_batch(views, "cuda")
+    torch.cuda.synchronize()
+    for (t, g), (sp_xyz, pc_idx, sp_t, mask) in zip(keep, outs):
+        assert np.array_equal(H(mask), g["mask"]), g.name
+        assert np.array_equal(H(pc_idx), g["pc_idx"]), g.name
+        assert np.array_equal(bits(H(sp_t)), bits(g["sp_t"])), g.name
+        assert np.array_equal(bits(H(sp_xyz)), bits(g["sp_xyz"])), g.name
+
+
+def _mixed_renderer(seed=3, sort=False):
+    mb = synth.make_mixed(n_clouds=4, n_views=10, seed=seed, size_range=(2e3, 3e5),
+                          resolutions=((64, 64), (96, 80), (200, 150), (256, 256)))
+    clouds = [D(c) for c in mb.clouds]
+    return batch.BatchRenderer(clouds, mb.views, mb.options, "cuda", sort=sort), mb
+
+
+@pytest.mark.parametrize("sort", [False, True])
+def test_mixed_batch_matches_per_view(sort):
+    r, mb = _mixed_renderer(sort=sort)
+    r.run()
+    torch.cuda.synchronize()
+    emitted = 0
+    for i, v in enumerate(r.views):
+        xyz = r.clouds[v.cloud]
+        sidx, sdep, hsh = ops.pts2plane(xyz, v.w2c, v.K, v.H, v.W, sort)
+        b_sidx, b_sdep, b_hash = r.hash_table(i)
+        assert torch.equal(sidx, b_sidx) and torch.equal(hsh, b_hash)
+        ref = ops.quick_sampling(xyz, v.c2w, v.fx, v.fy, v.cx, v.cy, v.W, v.H, mb.options, sidx, hsh)
+        _same(r.outputs(i), ref)
+        emitted += int(ref[3].sum())
+    assert emitted > 0
+
+
+def test_graph_replay_and_device_table():
+    r, _ = _mixed_renderer(seed=5)
+    r.run()
+    torch.cuda.synchronize()
+    first = [tuple(t.clone() for t in r.outputs(i)) for i in range(len(r.views))]
+    r.capture()
+    for _ in range(2):
+        for i in range(len(r.views)):
+            for t in r.outputs(i):
+                t.zero_()
+        r.replay()
+        torch.cuda.synchronize()
+        for i in range(len(r.views)):
+            _same(r.outputs(i), first[i])
+    r.release()
+
+
+def test_tuning_does_not_change_outputs():
+    r, _ = _mixed_renderer(seed=7)
+    r.run()
+    torch.cuda.synchronize()
+    first = [tuple(t.clone() for t in r.outputs(i)) for i in range(len(r.views))]
+    for heavy, blocks in [(1, 0), (64, 1), (160, 2), (320, 3)]:
+        r.tuning = native.HpTuning(heavy, blocks)
+        r.sample()
+        torch.cuda.synchronize()
+        for i in range(len(r.views)):
+            _same(r.outputs(i), first[i])
+
+
+def test_autotuner_caches_per_shape_class():
+    r, _ = _mixed_renderer(seed=9)
+    tuner = batch.Autotuner(reps=1)
+    choice = tuner.tune(r)
+    assert choice[0] in batch.Autotuner.HEAVY and choice[1] in batch.Autotuner.BLOCKS
+    assert tuner.cache[tuner.key(r)] == choice
+    assert tuner.tune(r) == choice
+    assert (r.tuning.heavy_window, r.tuning.blocks_per_sm) == choice
