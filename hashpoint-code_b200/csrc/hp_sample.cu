@@ -65,8 +65,8 @@ constexpr int kBinList = HP_BIN_LIST;  // distinct t-bins collected per candidat
 constexpr int kTeReg = 4;        // emitted sample depths kept in registers
 constexpr int kBallPass = 2;     // samples served by one ball-query walk
 constexpr int kHeavyWindow = 320;  // default: rays with more window candidates get a whole warp
-constexpr int kMaxHeavyWindow = 320;  // largest window a thread serves (its kept mask's size)
-constexpr int kMaskWords = (kMaxHeavyWindow + 31) / 32;  // kept-candidate mask of a thread-served ray
+constexpr int kMaxHeavyWindow = 4096;  // largest tunable threshold
+constexpr int kMaskWords = (kHeavyWindow + 31) / 32;  // kept-candidate mask of a thread-served ray (larger windows run unmasked)
 constexpr int kClasses = 64;     // window-size classes used to group a tile's rays
 constexpr int kWalkBatch = 4;    // bins whose sums one walk pass of a warp-served ray gathers
 
@@ -82,7 +82,7 @@ struct SampleArgs {
   int* __restrict__ pc_idx;
   float* __restrict__ sp_t;
   uint8_t* __restrict__ mask;
-  int heavy;  // rays with more window candidates than this are served by a whole warp (<= kMaxHeavyWindow)
+  int heavy;  // rays with more window candidates than this are served by a whole warp
 };
 
 struct Stage {
@@ -1001,7 +1001,7 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
       sc.work[i] = w;
       sc.item[i] = (t << 8) | ((vb - v0) << 4) | rows;
       if (sc.view) sc.view[i] = view;
-      atomicAdd(sc.counts + cost_class(w), 1);
+      atomicAdd(sc.counts + (sc.view ? view * 32 : 0) + cost_class(w), 1);
     }
     vb += rows;
   }
@@ -1026,6 +1026,46 @@ __global__ void __launch_bounds__(256) k_tile_order(Sched sc) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int c = cost_class(sc.work[i]);
     sc.order[base[c] + atomicAdd(sc.fill + c, 1)] = i;
+  }
+}
+
+// Batched queue order: view by view (in table order), heaviest class first
+// within a view, so only a view or two are in flight at a time -- their
+// points stay in L2 -- while one view's tail still overlaps the next view's
+// head.  base[v * 32 + c] = first queue position of view v's class-c items
+// (one block: exclusive scan over the n_views * 32 buckets).
+__global__ void __launch_bounds__(1024) k_batch_order_scan(Sched sc, int n_views, int* __restrict__ base) {
+  __shared__ int warp_sum[32];
+  const int n = n_views * 32;
+  const int per = (n + blockDim.x - 1) / blockDim.x;
+  const int b0 = threadIdx.x * per, b1 = min(n, b0 + per);
+  // bucket order: view ascending, class descending
+  auto at = [&](int r) { return (r / 32) * 32 + (31 - r % 32); };
+  int local = 0;
+  for (int r = b0; r < b1; r++) local += sc.counts[at(r)];
+  int incl = local;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_sum[warp] = incl;
+  __syncthreads();
+  int off = 0;
+  for (int w = 0; w < warp; w++) off += warp_sum[w];
+  int run = off + incl - local;
+  for (int r = b0; r < b1; r++) {
+    base[at(r)] = run;
+    run += sc.counts[at(r)];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_batch_order_place(Sched sc, const int* __restrict__ base) {
+  const int n = *sc.n_items;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int b = sc.view[i] * 32 + cost_class(sc.work[i]);
+    sc.order[base[b] + atomicAdd(sc.fill + b, 1)] = i;
   }
 }
 
@@ -1355,7 +1395,7 @@ static SchedLayout sched_layout(int64_t H, int64_t W) {
 // arguments, the views' first tiles and room for a copy of the view table.
 struct BatchLayout {
   SchedLayout q;
-  size_t args, tile_base, views, total;
+  size_t args, tile_base, views, buckets, total;
 };
 
 static BatchLayout batch_layout(int64_t total_tiles, int n_views) {
@@ -1366,11 +1406,12 @@ static BatchLayout batch_layout(int64_t total_tiles, int n_views) {
   B.q.order = 2 * per;
   B.q.view = 3 * per;
   B.q.small = 4 * per;
-  B.q.total = B.q.small + 512;
+  B.q.total = B.q.small + 512;  // next, n_items (counts and fill live in `buckets`)
   B.args = B.q.total;
   B.tile_base = B.args + align256s(sizeof(SampleArgs) * (size_t)n_views);
   B.views = B.tile_base + align256s(sizeof(int) * (size_t)(n_views + 1));
-  B.total = B.views + align256s(sizeof(hp_view) * (size_t)n_views);
+  B.buckets = B.views + align256s(sizeof(hp_view) * (size_t)n_views);  // counts, fill, base: n_views * 32 each
+  B.total = B.buckets + 3 * align256s(sizeof(int) * 32 * (size_t)n_views);
   return B;
 }
 
@@ -1552,20 +1593,26 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
   sc.item = (int*)(ws + B.q.item);
   sc.order = (int*)(ws + B.q.order);
   sc.view = (int*)(ws + B.q.view);
-  sc.counts = (int*)(ws + B.q.small);
-  sc.fill = sc.counts + 32;
-  sc.next = sc.counts + 64;
-  sc.n_items = sc.counts + 65;
+  const size_t bucket_bytes = align256s(sizeof(int) * 32 * (size_t)n_views);
+  sc.counts = (int*)(ws + B.buckets);
+  sc.fill = (int*)(ws + B.buckets + bucket_bytes);
+  int* base = (int*)(ws + B.buckets + 2 * bucket_bytes);
+  sc.next = (int*)(ws + B.q.small);
+  sc.n_items = sc.next + 1;
   SampleArgs* args = (SampleArgs*)(ws + B.args);
   int* tile_base = (int*)(ws + B.tile_base);
-  if (cudaMemsetAsync(sc.counts, 0, 512, st) != cudaSuccess) return set_error(HP_ERR_CUDA, "%s: memset failed", who);
+  if (cudaMemsetAsync(ws + B.q.small, 0, 512, st) != cudaSuccess ||
+      cudaMemsetAsync(ws + B.buckets, 0, 2 * bucket_bytes, st) != cudaSuccess)
+    return set_error(HP_ERR_CUDA, "%s: memset failed", who);
   k_batch_setup<<<1, 32, 0, st>>>(views_device, n_views, heavy, args, tile_base);
   if (int32_t rc = check_launch("k_batch_setup")) return rc;
   const int nt = (int)total_tiles;
   k_batch_tile_work<<<(nt + 7) / 8, 256, 0, st>>>(args, tile_base, n_views, nt, sc);
   if (int32_t rc = check_launch("k_batch_tile_work")) return rc;
-  k_tile_order<<<(nt + 255) / 256 < 148 ? (nt + 255) / 256 : 148, 256, 0, st>>>(sc);
-  if (int32_t rc = check_launch("k_tile_order")) return rc;
+  k_batch_order_scan<<<1, 1024, 0, st>>>(sc, n_views, base);
+  if (int32_t rc = check_launch("k_batch_order_scan")) return rc;
+  k_batch_order_place<<<(nt + 255) / 256 < 148 ? (nt + 255) / 256 : 148, 256, 0, st>>>(sc, base);
+  if (int32_t rc = check_launch("k_batch_order_place")) return rc;
   k_quick_sampling_batch<<<blocks < nt ? blocks : nt, kThreads, sizeof(Stage), st>>>(args, sc);
   return check_launch("k_quick_sampling_batch");
 }

@@ -186,6 +186,8 @@ class Server:
         return output_bytes(req, self.store.options) + self.store.entry_bytes(req)
 
     def _launch(self, reqs, slot, t0_event):
+        # heavy views first: the batch takes its views' tiles in table order
+        reqs = sorted(reqs, key=lambda r: -self.store.clouds[r.scene].shape[0])
         s = self.streams[slot]
         opt = self.store.options
         hold = []  # tensors that must live until the batch is done

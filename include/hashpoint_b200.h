@@ -148,7 +148,7 @@ HP_API size_t hp_quick_sampling_workspace_size(int32_t height, int32_t width);
 
 /* Launch tuning of hp_quick_sampling_batch (NULL or 0 fields = defaults).
  * Outputs never depend on it.  heavy_window: rays whose window holds more
- * candidates are served by a whole warp instead of one thread (0..320;
+ * candidates are served by a whole warp instead of one thread (0..4096;
  * default 320).  blocks_per_sm: resident blocks of the persistent sampling
  * kernel per SM (default: as many as fit). */
 typedef struct hp_tuning {
@@ -173,8 +173,9 @@ typedef struct hp_view {
 } hp_view;
 
 /* hp_quick_sampling for many views -- different clouds, cameras, image sizes
- * and options -- in one persistent launch over the tiles of all views
- * (heaviest first), so one view's tail overlaps the other views' work.  Each
+ * and options -- in one persistent launch over the tiles of all views, so one
+ * view's tail overlaps the next views' work.  Tiles are taken view by view in
+ * table order (heaviest first within a view), so put heavy views first.  Each
  * view's outputs are bit-identical to hp_quick_sampling's for that view.  No
  * counterpart call in the reference, which launches quick_sampling once per
  * view (epcq/csrc/epcq_render_topk.cu:341-417).  `views` (host) is checked and

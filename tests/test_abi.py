@@ -143,7 +143,7 @@ def test_batch_workspace_and_validation(L):
     assert "view 1" in _err(L) and "kernel_size" in _err(L)
     assert L.hp_quick_sampling_batch(two, None, 0, ctypes.byref(t), ws, 1 << 30, None) == -1
     assert L.hp_quick_sampling_batch(two, None, 2, ctypes.byref(t), ws, b - 1, None) == -2
-    assert L.hp_quick_sampling_batch(two, None, 2, ctypes.byref(native.HpTuning(321, 0)), ws, b, None) == -1
+    assert L.hp_quick_sampling_batch(two, None, 2, ctypes.byref(native.HpTuning(4097, 0)), ws, b, None) == -1
     assert "tuning" in _err(L)
 
 
