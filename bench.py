@@ -14,6 +14,13 @@ written to HBM.  With N GPUs (torchrun) every rank renders its own 100 views
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
+Beside the plain per-view figure the line carries the two system forms, run on
+one GPU only: "batched" (the same 100 views as one CUDA-graph-captured
+persistent launch, and an uneven 64-view batch over 8 clouds of 50k-4M points
+at 256^2..1600x1200) and "served" (16 resident scenes, 40M points, Poisson
+requests, continuous batching, p50/p99 latency), each against the plain
+per-view launches of the same kernels.
+
 --impl reference times the reference algorithm's CPU implementation (the
 oracle port, oracle/hp_oracle.cpp) on this machine's host cores on a bounded
 sample of the same workload, rank 0 only.
@@ -43,6 +50,8 @@ def parse():
     ap.add_argument("--impl", default="hashpoint", choices=["hashpoint", "reference"])
     ap.add_argument("--views", type=int, default=100)
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-systems", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--serve-requests", type=int, default=1000)
     return ap.parse_args()
 
 
@@ -245,6 +254,16 @@ def run_gpu(args):
     # end to end through the epcq API with host buffers
     e2e = run_e2e(args, sc, dev, pipe_hw=HW)
 
+    # the two system forms beside the plain per-view launch (one GPU runs them alone)
+    batched = served = None
+    if world == 1 and not args.no_systems:
+        del pipe
+        torch.cuda.empty_cache()
+        batched = run_batched(args, dev, xyz, sc, flush)
+        torch.cuda.empty_cache()
+        served = run_served(args, dev)
+        torch.cuda.empty_cache()
+
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -260,6 +279,10 @@ def run_gpu(args):
         "wall_s_timed_region": t_wall,
         "stages_ms_per_view": {"build_plus_sample": ms_per_step / len(structs), "sample": samp_avg_ms},
     }
+    if batched is not None:
+        result["batched"] = batched
+    if served is not None:
+        result["served"] = served
     if rank == 0 and world == 1:
         result["cpu_baseline"] = cpu_baseline()
     if world > 1:
@@ -320,6 +343,111 @@ def run_e2e(args, sc, dev, pipe_hw):
             "d2h_bytes_per_step": d2h, "ms_per_step": ms, "api": "epcq.NeuralPoints.pts2plane + "
             "render_image_hashtable_topk per view, xyz and cameras copied from pinned host memory each step, "
             "per-view emitted-sample counts read back"}
+
+
+def _event_ms(fn, reps, flush=None):
+    import torch
+    ts = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def run_batched(args, dev, xyz, sc, flush):
+    """Batching: the same 100 views as one graph-captured persistent launch; and the uneven
+    multi-cloud batch (64 views over 8 clouds of 50k-4M points at 256^2..1600x1200), each
+    against the plain per-view launches of the same kernels over the same buffers."""
+    import torch
+
+    from hashpoint import batch, synth
+
+    out = {}
+    tuner = batch.Autotuner()
+    # same workload as the headline: 100 views of the 1M-point cloud, one batch
+    r = batch.BatchRenderer([xyz], [(0, c) for c in sc.cameras], sc.options, dev)
+    tuning = tuner.tune(r)
+    r.capture()
+    r.run_per_view()
+    torch.cuda.synchronize(dev)
+    pv = _event_ms(r.run_per_view, 3, flush)
+    g = _event_ms(r.replay, max(args.steps, 3), flush)
+    out["shapes_100views"] = {"rays_per_s": r.rays / (g * 1e-3), "ms": g, "per_view_rays_s": r.rays / (pv * 1e-3),
+                              "per_view_ms": pv, "speedup": pv / g, "tuning": list(tuning),
+                              "path": "hp_pts2plane x100 on 4 streams + one hp_quick_sampling_batch, CUDA graph"}
+    r.release()
+    del r
+    torch.cuda.empty_cache()
+    # uneven batch: 8 clouds log-uniform in 50k-4M points, 64 views, mixed resolutions
+    mb = synth.make_mixed(n_clouds=8, n_views=64, seed=0)
+    clouds = [torch.from_numpy(c).to(dev) for c in mb.clouds]
+    order = sorted(range(len(mb.views)), key=lambda i: -len(mb.clouds[mb.views[i][0]]))  # heavy views first
+    r = batch.BatchRenderer(clouds, [mb.views[i] for i in order], mb.options, dev)
+    tuning = tuner.tune(r)
+    r.capture()
+    r.run_per_view()
+    torch.cuda.synchronize(dev)
+    pv = _event_ms(r.run_per_view, 3, flush)
+    g = _event_ms(r.replay, max(args.steps, 3), flush)
+    out["mixed_64views_8clouds"] = {
+        "rays_per_s": r.rays / (g * 1e-3), "ms": g, "per_view_rays_s": r.rays / (pv * 1e-3), "per_view_ms": pv,
+        "speedup": pv / g, "tuning": list(tuning), "rays": r.rays, "points": [int(c.shape[0]) for c in clouds],
+        "path": "one CUDA graph: 64 hash-table builds on 4 streams + one persistent sampling launch"}
+    r.release()
+    del r, clouds
+    return out
+
+
+def run_served(args, dev):
+    """Serving: 16 resident scenes (40M points), Poisson requests at 2000/s (mixed resolutions,
+    K=8), 120 GB budget, continuous batching; p50/p99 latency and rays/s against serial plain
+    launches of the same requests (hash tables cached per scene, camera pose and resolution)."""
+    import numpy as np
+    import torch
+
+    from hashpoint import ops, serve, synth
+
+    clouds, poses = serve.make_scenes(np.random.default_rng(0))
+    opt = synth.Options(kernel_size=5, radius_threshold=0.008, num_sample_points_per_ray=8, num_point_cloud_per_sp=8)
+    store = serve.SceneStore([torch.from_numpy(c).to(dev) for c in clouds], poses, opt, dev)
+    n = max(int(args.serve_requests), 10)
+
+    def requests(rate, count):
+        return serve.poisson_requests(np.random.default_rng(1), count, rate, len(clouds), len(poses[0]),
+                                      synth.MIXED_RESOLUTIONS)
+
+    budget = 120 << 30
+    serve.Server(store, budget).run(requests(2000.0, n))  # warm: hash-table cache and allocator
+    hot = serve.Server(store, budget).run(requests(2000.0, n))
+    light = serve.Server(store, budget).run(requests(200.0, max(n // 3, 10)))
+    # the same requests through serial plain launches (cached tables, one request at a time)
+    reqs = requests(2000.0, n)
+    mk = lambda b: torch.empty(max(b, 1), dtype=torch.uint8, device=dev)
+
+    def serial():
+        s = torch.cuda.current_stream(dev)
+        for q in reqs:
+            e = store.lookup(q, s, mk)
+            e.users -= 1
+            cam, c2w, _, _ = store.camera(q.scene, q.pose, q.width, q.height)
+            ops.quick_sampling(store.clouds[q.scene], c2w, cam.fx, cam.fy, cam.cx, cam.cy, q.width, q.height, opt,
+                               e.sidx, e.hash)
+
+    ser = _event_ms(serial, 1)
+    rays = sum(q.rays for q in reqs)
+    keep = ("requests", "done", "rejected", "batches", "p50_ms", "p99_ms", "mean_ms", "rays_per_s", "span_ms")
+    return {"scenes": len(clouds), "points": int(sum(len(c) for c in clouds)), "budget_gb": 120,
+            "lambda_2000": {k: hot[k] for k in keep}, "lambda_200": {k: light[k] for k in keep},
+            "serial_plain_rays_per_s": rays / (ser * 1e-3), "serial_plain_ms": ser,
+            "speedup_vs_serial_plain": (hot["rays_per_s"] or 0) / (rays / (ser * 1e-3)),
+            "note": "at 2000 requests/s the offered load exceeds the GPU's capacity, so latency is mostly "
+                    "queueing; 200 requests/s is below it"}
 
 
 def run_reference(args):

@@ -124,6 +124,28 @@ class BatchRenderer:
         self.build()
         self.sample()
 
+    def run_per_view(self):
+        """The plain per-view launch over the same buffers, for comparison: hp_pts2plane then
+        hp_quick_sampling, one view at a time on the current stream."""
+        L = native.lib()
+        st = _vp(torch.cuda.current_stream(self.device).cuda_stream)
+        if getattr(self, "_pv_ws", None) is None:
+            need = max(L.hp_quick_sampling_workspace_size(v.H, v.W) for v in self.views)
+            self._pv_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+            self._pv_opt = ops.make_options(self.options)
+        ws = self._pv_ws
+        for v in self.views:
+            xyz = self.clouds[v.cloud]
+            rc = L.hp_pts2plane(_vp(xyz.data_ptr()), v.n, ctypes.byref(v.cam), v.sort, _vp(v.sidx.data_ptr()),
+                                _vp(v.sdep.data_ptr()), _vp(v.hash.data_ptr()), _vp(v.ws.data_ptr()), v.ws_bytes, st)
+            native.check(rc, "hp_pts2plane")
+            sp_xyz, pc_idx, sp_t, mask = v.out
+            rc = L.hp_quick_sampling(_vp(xyz.data_ptr()), v.n, ctypes.byref(v.cam), ctypes.byref(self._pv_opt),
+                                     _vp(v.sidx.data_ptr()), v.n, _vp(v.hash.data_ptr()), _vp(sp_xyz.data_ptr()),
+                                     _vp(pc_idx.data_ptr()), _vp(sp_t.data_ptr()), _vp(mask.data_ptr()),
+                                     _vp(ws.data_ptr()), ws.numel(), st)
+            native.check(rc, "hp_quick_sampling")
+
     # -- CUDA graph -----------------------------------------------------------
     def capture(self):
         """Capture build + sample as one CUDA graph (run once eagerly first to load the kernels)."""
