@@ -10,6 +10,9 @@ signatures for the search+sample path:
     .render_image_hashtable_topk(cam, opt, idx, depth, hash)      (:297-327)
         -> sp_xyz f32[H,W,S,3], pc_idx int32[H,W,S,P], sp_t f32[H,W,S], mask bool[H,W,S]
 
+  FeatureQuery().forward(neuralpoints, sp_xyz, pc_idx, mask, cam, ray_index_uv) (:328-387)
+  clamp_t(t_val, vsize), render(deltas, sigmas, rgbs, white_bg)   (:508-529)
+
 pts2plane runs the projection, the per-pixel counting sort and the bucket
 order in the CUDA library (one call, no torch.sort); render_image_hashtable_topk
 runs the fused search/sample kernel.  Both launch on torch's current stream.
@@ -257,3 +260,46 @@ class NeuralPoints(nn.Module):
             cam._save2torch(os.path.join(out_dir, "cam.pt"))
             opt._save2torch(os.path.join(out_dir, "opt.pt"))
         return self.quick_sampling(self._to_cpp(), cam._to_cpp(), opt._to_cpp(), sorted_point_idx_list, hashtable)
+
+
+class FeatureQuery(nn.Module):
+    """Per-sample point attributes for the aggregator (epcq.py:328-387).
+
+    forward gathers, for every sample whose mask is set, the xyz / rgb / dir /
+    feat rows of its P point ids (zeros where the id is -1), its sample point
+    and the direction of its pixel ray -- the same seven tensors as the
+    reference, produced by one CUDA gather after a scan of the mask."""
+
+    def generate_rays(self, cam: CameraSpec):
+        """(rays_o, rays_d) [H, W, 3] through pixel corners, as the reference builds them (epcq.py:333-341)."""
+        dev = cam.c2w.device
+        fx, fy, cx, cy = (float(_scalar(v)) for v in (cam.fx, cam.fy, cam.cx, cam.cy))
+        W, H = int(_scalar(cam.width)), int(_scalar(cam.height))
+        y, x = torch.meshgrid(torch.arange(H, dtype=torch.float32, device=dev),
+                              torch.arange(W, dtype=torch.float32, device=dev), indexing="ij")
+        d = torch.stack([(x - cx) / fx, (y - cy) / fy, torch.ones_like(x)], dim=-1)
+        rays_d = torch.sum(d[:, :, None, :] * cam.c2w[:3, :3][None, None, :, :], dim=-1)
+        rays_o = cam.c2w[:3, 3].expand_as(rays_d)
+        return rays_o, rays_d
+
+    def forward(self, neuralpoints, output_sp_xyz: torch.Tensor, output_pc_idx: torch.Tensor,
+                mask_out: torch.Tensor, cam: CameraSpec, ray_index_uv: torch.Tensor = None):
+        """-> (pc_xyz, pc_rgb, pc_dir, pc_feat, output_sp_xyz, valid_sp_mask_out, rays_d) for the M valid samples."""
+        uv = ray_index_uv if ray_index_uv is not None and len(ray_index_uv) != 0 else None
+        pc_idx = output_pc_idx if output_pc_idx.dtype == torch.int32 else output_pc_idx.to(torch.int32)
+        feat = neuralpoints.feat_data.detach()
+        return ops.feature_query(neuralpoints.xyz_data.detach().contiguous(), neuralpoints.rgb_data.detach().contiguous(),
+                                 neuralpoints.dir_data.detach().contiguous(), feat.contiguous(),
+                                 output_sp_xyz.contiguous(), pc_idx.contiguous(), mask_out, cam.c2w,
+                                 _scalar(cam.fx), _scalar(cam.fy), _scalar(cam.cx), _scalar(cam.cy),
+                                 _scalar(cam.width), uv)
+
+
+def clamp_t(t_val, vsize=0.004):
+    """Sample spacings with out-of-range gaps set to vsize (epcq.py:508-515), on the GPU."""
+    return ops.clamp_t(t_val.contiguous(), vsize)
+
+
+def render(deltas, sigmas, rgbs, white_bg=False):
+    """Front-to-back compositing of [R, S] samples into [R, 3] colours (epcq.py:517-529), on the GPU."""
+    return ops.render(deltas.contiguous(), sigmas.contiguous(), rgbs.contiguous(), white_bg)

@@ -24,7 +24,7 @@ LIB_NAME = "libhashpoint_b200.so"
 LIB_PATH = os.path.join(LIB_DIR, LIB_NAME)
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
-SOURCES = ["hp_api.cu", "hp_build.cu", "hp_sample.cu", "hp_query.cu"]
+SOURCES = ["hp_api.cu", "hp_build.cu", "hp_sample.cu", "hp_query.cu", "hp_feature.cu"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 
@@ -32,7 +32,8 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
 EXPORTS = ["hp_version", "hp_last_error", "hp_projection_rounding", "hp_pts2plane_workspace_size", "hp_pts2plane",
            "hp_pts2plane_noalloc", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling",
            "hp_quick_sampling_batch_workspace_size", "hp_quick_sampling_batch", "hp_quick_query_for_nearby_point",
-           "hp_scatter", "hp_ray_directions"]
+           "hp_scatter", "hp_ray_directions", "hp_mask_scan", "hp_mask_scan_workspace_size", "hp_feature_query",
+           "hp_clamp_t", "hp_render"]
 
 HP_OK = 0
 
@@ -104,6 +105,11 @@ class HpOptions(ctypes.Structure):
                 ("sdf2weight_gaussian_alpha", ctypes.c_float), ("sdf2weight_gaussian_gamma", ctypes.c_float)]
 
 
+class HpPointAttrs(ctypes.Structure):
+    _fields_ = [("xyz", ctypes.c_void_p), ("rgb", ctypes.c_void_p), ("dir", ctypes.c_void_p), ("feat", ctypes.c_void_p),
+                ("feat_dim", ctypes.c_int32), ("feat_half", ctypes.c_int32), ("n_points", ctypes.c_int64)]
+
+
 class HpTuning(ctypes.Structure):
     """Launch tuning of hp_quick_sampling_batch (0 = default)."""
     _fields_ = [("heavy_window", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32)]
@@ -156,6 +162,17 @@ def lib():
         L.hp_quick_sampling_batch_workspace_size.restype = sz
         L.hp_quick_sampling_batch.argtypes = [view_p, vp, i32, ctypes.POINTER(HpTuning), vp, sz, vp]
         L.hp_quick_sampling_batch.restype = i32
+        L.hp_mask_scan.argtypes = [vp, i64, vp, vp, vp, sz, vp]
+        L.hp_mask_scan.restype = i32
+        L.hp_mask_scan_workspace_size.argtypes = [i64]
+        L.hp_mask_scan_workspace_size.restype = sz
+        L.hp_feature_query.argtypes = [ctypes.POINTER(HpPointAttrs), vp, vp, vp, i64, i32, i32, vp, cam_p, vp,
+                                       vp, vp, vp, vp, vp, vp, vp, vp]
+        L.hp_feature_query.restype = i32
+        L.hp_clamp_t.argtypes = [vp, i64, i32, ctypes.c_float, vp, vp]
+        L.hp_clamp_t.restype = i32
+        L.hp_render.argtypes = [vp, vp, ctypes.c_float, vp, vp, i64, i32, i32, vp, vp]
+        L.hp_render.restype = i32
         L.hp_quick_query_for_nearby_point.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, i64, vp, vp]
         L.hp_quick_query_for_nearby_point.restype = i32
         L.hp_scatter.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp]

@@ -241,3 +241,98 @@ def ray_directions(c2w, fx, fy, cx, cy, width, height):
     rc = native.lib().hp_ray_directions(ctypes.byref(cam), _ptr(out), _stream(c2w.device))
     native.check(rc, "hp_ray_directions")
     return out
+
+
+# ---------------------------------------------------------------------------
+# downstream of sampling: FeatureQuery gather, clamp_t, render
+# ---------------------------------------------------------------------------
+def mask_scan(mask):
+    """(offsets int32 [n], count int32 [1]) of a bool/uint8 mask: the exclusive scan of its set entries."""
+    check_input(mask, "mask")
+    if mask.dtype not in (torch.bool, torch.uint8):
+        raise RuntimeError("mask must be bool or uint8")
+    n = mask.numel()
+    dev = mask.device
+    offsets = torch.empty(n, dtype=torch.int32, device=dev)
+    count = torch.empty(1, dtype=torch.int32, device=dev)
+    L = native.lib()
+    ws_bytes = L.hp_mask_scan_workspace_size(n)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    rc = L.hp_mask_scan(_ptr(mask), n, _ptr(offsets), _ptr(count), _ptr(ws), ws_bytes, _stream(dev))
+    native.check(rc, "hp_mask_scan")
+    return offsets, count
+
+
+def feature_query(xyz, rgb, dir_, feat, sp_xyz, pc_idx, mask, c2w, fx, fy, cx, cy, width, ray_uv=None):
+    """FeatureQuery.forward's gather (epcq/epcq.py:345-387) on the GPU.
+
+    Returns (pc_xyz [M,P,3], pc_rgb [M,P,3], pc_dir [M,P,3], pc_feat [M,P,F] f32, sp_xyz [M,3],
+    valid bool [M,P], rays_d [M,3]) for the M samples whose mask is set.  The sample count is read
+    back to size the outputs (one host synchronisation, as the reference's boolean indexing does)."""
+    for t, nme in ((xyz, "xyz_data"), (rgb, "rgb_data"), (dir_, "dir_data"), (sp_xyz, "output_sp_xyz")):
+        check_input(t, nme, torch.float32)
+    check_input(feat, "feat_data")
+    if feat.dtype not in (torch.float32, torch.float16):
+        raise RuntimeError("feat_data must be float32 or float16")
+    check_input(pc_idx, "output_pc_idx", torch.int32)
+    check_matrix(c2w, "c2w")
+    S, P = int(pc_idx.shape[-2]), int(pc_idx.shape[-1])
+    n_rays = pc_idx.numel() // max(S * P, 1)
+    if mask.numel() != n_rays * S or sp_xyz.numel() != n_rays * S * 3:
+        raise RuntimeError("mask_out / output_sp_xyz do not match output_pc_idx")
+    if ray_uv is not None:
+        ray_uv = ray_uv.to(device=xyz.device, dtype=torch.int32).contiguous()
+        if ray_uv.shape != (n_rays, 2):
+            raise RuntimeError("ray_index_uv must be [rays, 2] (u, v)")
+    mask = mask.contiguous()
+    offsets, count = mask_scan(mask)
+    M = int(count.item())
+    dev = xyz.device
+    F = int(feat.shape[-1]) if feat.dim() == 2 else 0
+    out = (torch.empty((M, P, 3), dtype=torch.float32, device=dev), torch.empty((M, P, 3), dtype=torch.float32, device=dev),
+           torch.empty((M, P, 3), dtype=torch.float32, device=dev), torch.empty((M, P, F), dtype=torch.float32, device=dev),
+           torch.empty((M, 3), dtype=torch.float32, device=dev), torch.empty((M, P), dtype=torch.bool, device=dev),
+           torch.empty((M, 3), dtype=torch.float32, device=dev))
+    if M == 0:
+        return out
+    pts = native.HpPointAttrs(_ptr(xyz).value, _ptr(rgb).value, _ptr(dir_).value, _ptr(feat).value, F,
+                              int(feat.dtype == torch.float16), xyz.shape[0])
+    cam = make_camera(c2w=c2w, fx=fx, fy=fy, cx=cx, cy=cy, width=width, height=1)
+    rc = native.lib().hp_feature_query(ctypes.byref(pts), _ptr(sp_xyz), _ptr(pc_idx), _ptr(mask), n_rays, S, P,
+                                       _ptr(offsets), ctypes.byref(cam), _ptr(ray_uv), *[_ptr(t) for t in out[:4]],
+                                       _ptr(out[4]), _ptr(out[5]), _ptr(out[6]), _stream(dev))
+    native.check(rc, "hp_feature_query")
+    return out
+
+
+def clamp_t(t_val, vsize=0.004):
+    """clamp_t (epcq/epcq.py:508-515) on the GPU: t_val [R, S] -> t_dist [R, S]."""
+    check_input(t_val, "t_val", torch.float32)
+    R, S = t_val.shape
+    out = torch.empty_like(t_val)
+    rc = native.lib().hp_clamp_t(_ptr(t_val), R, S, float(vsize), _ptr(out), _stream(t_val.device))
+    native.check(rc, "hp_clamp_t")
+    return out
+
+
+def render(deltas, sigmas, rgbs, white_bg=False, t_val=None, vsize=0.004):
+    """render (epcq/epcq.py:517-529) on the GPU: colour [R, 3].  With deltas None, the spacings are
+    clamp_t(t_val, vsize), computed inside the same kernel."""
+    check_input(sigmas, "sigmas", torch.float32)
+    check_input(rgbs, "rgbs", torch.float32)
+    R, S = sigmas.shape
+    if rgbs.shape != (R, S, 3):
+        raise RuntimeError("rgbs must be [rays, samples, 3]")
+    if deltas is not None:
+        check_input(deltas, "deltas", torch.float32)
+        if deltas.shape != (R, S):
+            raise RuntimeError("deltas must match sigmas")
+    elif t_val is None or tuple(t_val.shape) != (R, S):
+        raise RuntimeError("render needs deltas or t_val of the sigmas' shape")
+    else:
+        check_input(t_val, "t_val", torch.float32)
+    color = torch.empty((R, 3), dtype=torch.float32, device=sigmas.device)
+    rc = native.lib().hp_render(_ptr(deltas), _ptr(t_val), float(vsize), _ptr(sigmas), _ptr(rgbs), R, S,
+                                int(bool(white_bg)), _ptr(color), _stream(sigmas.device))
+    native.check(rc, "hp_render")
+    return color

@@ -142,6 +142,56 @@ HP_API int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const hp_ca
                                  float* sp_xyz, int32_t* pc_idx, float* sp_t, uint8_t* mask, void* workspace,
                                  size_t workspace_bytes, hp_stream_t stream);
 
+/* Point attributes read by hp_feature_query: xyz, rgb, dir f32 [n_points, 3]
+ * and feat [n_points, feat_dim] in f32 or (feat_half != 0) f16. */
+typedef struct hp_point_attrs {
+  const float* xyz;
+  const float* rgb;
+  const float* dir;
+  const void* feat;
+  int32_t feat_dim;
+  int32_t feat_half;
+  int64_t n_points;
+} hp_point_attrs;
+
+/* offsets[i] = number of nonzero bytes of mask[0..i) (an exclusive scan), and
+ * *count (device) = all of them.  Numbers the valid samples for
+ * hp_feature_query, in place of the reference's boolean indexing
+ * (epcq/epcq.py:347-351).  workspace: hp_mask_scan_workspace_size(n) bytes. */
+HP_API int32_t hp_mask_scan(const uint8_t* mask, int64_t n, int32_t* offsets, int32_t* count, void* workspace,
+                            size_t workspace_bytes, hp_stream_t stream);
+HP_API size_t hp_mask_scan_workspace_size(int64_t n);
+
+/* FeatureQuery.forward (epcq/epcq.py:345-387): for every sample with mask set
+ * (n_rays x S samples; offsets from hp_mask_scan give its output row m), write
+ * out_sp_xyz[m] = sp_xyz of the sample, rays_d[m] = the direction of its
+ * pixel ray as generate_rays builds it (epcq.py:333-341: ((u - cx) / fx,
+ * (v - cy) / fy, 1) times the rotation of cam->c2w, pixel corners, not
+ * centres), and for each of its P ids: valid[m, p] and the id's xyz / rgb /
+ * dir / feat rows in pc_xyz / pc_rgb / pc_dir [M, P, 3] and pc_feat
+ * [M, P, feat_dim] (f32), or zeros for an id of -1 (any id outside
+ * [0, n_points) is treated as -1).  ray_uv: [n_rays, 2] (u, v) of each ray
+ * (the reference's ray_index_uv), or NULL for the image's pixels in row-major
+ * order (then cam->width is used). */
+HP_API int32_t hp_feature_query(const hp_point_attrs* pts, const float* sp_xyz, const int32_t* pc_idx,
+                                const uint8_t* mask, int64_t n_rays, int32_t S, int32_t P, const int32_t* offsets,
+                                const hp_camera* cam, const int32_t* ray_uv, float* pc_xyz, float* pc_rgb,
+                                float* pc_dir, float* pc_feat, float* out_sp_xyz, uint8_t* valid, float* rays_d,
+                                hp_stream_t stream);
+
+/* clamp_t (epcq/epcq.py:508-515): t_dist[r, s] = t[r, s+1] - t[r, s], the
+ * last one vsize, and any gap below 1e-8 or above 2 * vsize replaced by vsize. */
+HP_API int32_t hp_clamp_t(const float* t_val, int64_t n_rays, int32_t S, float vsize, float* t_dist,
+                          hp_stream_t stream);
+
+/* render (epcq/epcq.py:517-529): colour [n_rays, 3] of sigmas [n_rays, S] and
+ * rgbs [n_rays, S, 3] composited front to back with the spacings `deltas`
+ * [n_rays, S] -- or, when deltas is NULL, with clamp_t(t_val, vsize) computed
+ * on the fly -- over a black (white_bg = 0) or white background. */
+HP_API int32_t hp_render(const float* deltas, const float* t_val, float vsize, const float* sigmas,
+                         const float* rgbs, int64_t n_rays, int32_t S, int32_t white_bg, float* color,
+                         hp_stream_t stream);
+
 /* Scratch bytes hp_quick_sampling needs for an image of this size (its tile
  * schedule); workspace must be 256-byte aligned. */
 HP_API size_t hp_quick_sampling_workspace_size(int32_t height, int32_t width);

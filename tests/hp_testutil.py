@@ -11,7 +11,17 @@ GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def golden_files():
-    return sorted(glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    """Search+sample fixtures (make_golden.py)."""
+    return sorted(f for f in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")) if not os.path.basename(f).startswith("fd_"))
+
+
+def downstream_files(kind):
+    """FeatureQuery / render fixtures (make_golden_downstream.py) of a kind ('feature' or 'render')."""
+    out = []
+    for f in sorted(glob.glob(os.path.join(GOLDEN_DIR, "fd_*.npz"))):
+        if str(np.load(f)["kind"]) == kind:
+            out.append(f)
+    return out
 
 
 def golden_names():
