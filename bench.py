@@ -255,8 +255,9 @@ def run_gpu(args):
     e2e = run_e2e(args, sc, dev, pipe_hw=HW)
 
     # the two system forms beside the plain per-view launch (one GPU runs them alone)
-    batched = served = None
+    batched = served = downstream = None
     if world == 1 and not args.no_systems:
+        downstream = run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
         del pipe
         torch.cuda.empty_cache()
         batched = run_batched(args, dev, xyz, sc, flush)
@@ -279,6 +280,8 @@ def run_gpu(args):
         "wall_s_timed_region": t_wall,
         "stages_ms_per_view": {"build_plus_sample": ms_per_step / len(structs), "sample": samp_avg_ms},
     }
+    if downstream is not None:
+        result["downstream"] = downstream
     if batched is not None:
         result["batched"] = batched
     if served is not None:
@@ -358,6 +361,61 @@ def _event_ms(fn, reps, flush=None):
         e1.synchronize()
         ts.append(e0.elapsed_time(e1))
     return statistics.median(ts)
+
+
+def run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush):
+    """The rows after sampling on the same views: the FeatureQuery gather (mask scan + gather of
+    xyz/rgb/dir and the fp16[32] features of every selected point) and render (clamp_t fused),
+    timed per view with CUDA events; HBM fraction from the bytes each must move."""
+    import numpy as np
+    import torch
+
+    from hashpoint import ops
+
+    n = xyz.shape[0]
+    rng = np.random.default_rng(3)
+    rgb = torch.from_numpy(rng.random((n, 3), dtype=np.float32)).to(dev)
+    dr = torch.from_numpy(rng.standard_normal((n, 3)).astype(np.float32)).to(dev)
+    S, P, F = sc.options.num_sample_points_per_ray, sc.options.num_point_cloud_per_sp, feat.shape[1]
+    fq_ms, fq_bytes, r_ms, r_bytes = [], [], [], []
+    with torch.cuda.stream(stream):
+        for i in range(min(10, len(structs))):
+            pipe.render(xyz, structs[i], stream)
+            c = sc.cameras[i]
+            sp_xyz, pc_idx, sp_t, mask = (t.clone() for t in (pipe.sp_xyz, pipe.pc_idx, pipe.sp_t, pipe.mask))
+            c2w = torch.from_numpy(c.c2w).to(dev)
+            R = c.width * c.height
+            sig = torch.rand((R, S), device=dev) * 50
+            rgbs = torch.rand((R, S, 3), device=dev)
+            t_val = sp_t.view(R, S)
+            for rep in range(2):  # the second is timed
+                flush.fill_(1)
+                e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+                e[0].record(stream)
+                out = ops.feature_query(xyz, rgb, dr, feat, sp_xyz, pc_idx, mask, c2w, c.fx, c.fy, c.cx, c.cy, c.width)
+                e[1].record(stream)
+                flush.fill_(1)
+                e[2].record(stream)
+                ops.render(None, sig, rgbs, t_val=t_val)
+                e[3].record(stream)
+                stream.synchronize()
+            M = out[0].shape[0]
+            # mask read, offsets written and read, sample rows and ids read, P ids' rows gathered, outputs written
+            fq_bytes.append(R * S * (1 + 8) + M * (12 + 4 * P) + M * P * (36 + 2 * F) +
+                            M * (P * (36 + 4 * F + 1) + 24))
+            fq_ms.append(e[0].elapsed_time(e[1]))
+            r_bytes.append(R * S * (4 + 4 + 12) + R * 12)
+            r_ms.append(e[2].elapsed_time(e[3]))
+    fq = statistics.median(fq_ms)
+    rr = statistics.median(r_ms)
+    fqb = sum(fq_bytes) / len(fq_bytes)
+    rb = sum(r_bytes) / len(r_bytes)
+    return {"feature_query": {"ms_per_view": fq, "bytes_per_view": fqb, "gbs": fqb / (fq * 1e-3) / 1e9,
+                              "frac_of_hbm": fqb / (fq * 1e-3) / 1e9 / peak,
+                              "note": "includes the mask scan and the read-back of the sample count"},
+            "render": {"ms_per_view": rr, "bytes_per_view": rb, "gbs": rb / (rr * 1e-3) / 1e9,
+                       "frac_of_hbm": rb / (rr * 1e-3) / 1e9 / peak, "note": "clamp_t fused"},
+            "views": len(fq_ms)}
 
 
 def run_batched(args, dev, xyz, sc, flush):
