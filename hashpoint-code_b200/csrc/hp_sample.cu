@@ -73,6 +73,7 @@ constexpr int kWalkBatch = 4;    // bins whose sums one walk pass of a warp-serv
 struct SampleArgs {
   const float* __restrict__ xyz;
   const int* __restrict__ sidx;
+  const float4* __restrict__ pts;  // sorted_point_idx packed: (x, y, z, id as int bits; -1 = invalid)
   const int2* __restrict__ hash;
   int n_points;  // ids outside [0, n_points) are skipped
   int n_sorted;  // bucket ranges are clipped to [0, n_sorted)
@@ -125,13 +126,25 @@ struct SrcGlobal {
   __device__ __forceinline__ int2 range(const SampleArgs& a, int vv, int uu) const {
     return bucket_range(__ldg(a.hash + (size_t)vv * a.cam.width + uu), a.n_sorted);
   }
-  __device__ __forceinline__ float4 fetch(const SampleArgs& a, int j) const {
-    const int id = __ldg(a.sidx + j);
-    if ((unsigned)id >= (unsigned)a.n_points) return make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-    const float4 p = load_point(a.xyz, id);
-    return make_float4(p.x, p.y, p.z, __int_as_float(id));
-  }
+  __device__ __forceinline__ float4 fetch(const SampleArgs& a, int j) const { return __ldg(a.pts + j); }
 };
+
+// Pack the candidates once per launch: pts[j] = (xyz of sorted_point_idx[j],
+// its id), or id -1 when the id is outside [0, n_points).  Every later fetch
+// of candidate j -- staging or global -- is then one 16-byte load instead of
+// an id load and a dependent point gather.
+__global__ void k_pack_points(const int* __restrict__ sidx, int n_sorted, const float* __restrict__ xyz, int n_points,
+                              float4* __restrict__ pts) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_sorted) return;
+  const int id = __ldg(sidx + j);
+  float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+  if ((unsigned)id < (unsigned)n_points) {
+    const float4 q = load_point(xyz, id);
+    p = make_float4(q.x, q.y, q.z, __int_as_float(id));
+  }
+  pts[j] = p;
+}
 
 // Visit a ray's window candidates in the reference's order -- window rows
 // top to bottom, cells left to right (coordinates clamped into the image, so
@@ -1126,13 +1139,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
         else
           hi_c = mid;
       }
-      const int id = __ldg(a.sidx + st.start[lo_c] + (i - st.off[lo_c]));
-      float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-      if ((unsigned)id < (unsigned)a.n_points) {
-        const float4 q = load_point(a.xyz, id);
-        p = make_float4(q.x, q.y, q.z, __int_as_float(id));
-      }
-      st.cand[i] = p;
+      st.cand[i] = __ldg(a.pts + st.start[lo_c] + (i - st.off[lo_c]));
     }
     __syncthreads();
   }
@@ -1242,18 +1249,32 @@ __global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a, Sc
 
 // Device view table -> per-view kernel arguments and the first global tile of
 // each view (exclusive scan; tile_base[n_views] = all tiles).  One warp.
+// Also the first packed-point slot of each view (pack_base; regions padded to
+// 16 slots) and the views' packed-point arrays inside `pts`.
 __global__ void k_batch_setup(const hp_view* __restrict__ views, int n_views, int heavy,
-                              SampleArgs* __restrict__ args, int* __restrict__ tile_base) {
+                              SampleArgs* __restrict__ args, int* __restrict__ tile_base, int* __restrict__ pack_base,
+                              float4* __restrict__ pts) {
   const int lane = threadIdx.x;
-  int run = 0;
+  int run = 0, prun = 0;
   for (int b = 0; b < n_views; b += 32) {
     const int v = b + lane;
-    int tiles = 0;
+    int tiles = 0, slots = 0;
+    if (v < n_views) slots = ((int)views[v].n_sorted + 15) & ~15;
+    int pincl = slots;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, pincl, o);
+      if (lane >= o) pincl += t;
+    }
+    const int pfirst = prun + pincl - slots;
+    if (v < n_views) pack_base[v] = pfirst;
+    prun += __shfl_sync(0xffffffffu, pincl, 31);
     if (v < n_views) {
       const hp_view& hv = views[v];
       SampleArgs a;
       a.xyz = hv.xyz;
       a.sidx = hv.sorted_point_idx;
+      a.pts = pts + pfirst;
       a.hash = (const int2*)hv.hash_table;
       a.n_points = (int)hv.n_points;
       a.n_sorted = (int)hv.n_sorted;
@@ -1289,7 +1310,35 @@ __global__ void k_batch_setup(const hp_view* __restrict__ views, int n_views, in
     if (v < n_views) tile_base[v] = run + incl - tiles;
     run += __shfl_sync(0xffffffffu, incl, 31);
   }
-  if (lane == 0) tile_base[n_views] = run;
+  if (lane == 0) {
+    tile_base[n_views] = run;
+    pack_base[n_views] = prun;
+  }
+}
+
+// Pack every view's candidates (see k_pack_points); slot g of the batch.
+__global__ void k_batch_pack(const SampleArgs* __restrict__ args, const int* __restrict__ pack_base, int n_views,
+                             int total) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  int lo = 0, hi = n_views;  // pack_base[lo] <= g < pack_base[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pack_base[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const SampleArgs& a = args[lo];
+  const int j = g - pack_base[lo];
+  if (j >= a.n_sorted) return;
+  const int id = __ldg(a.sidx + j);
+  float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+  if ((unsigned)id < (unsigned)a.n_points) {
+    const float4 q = load_point(a.xyz, id);
+    p = make_float4(q.x, q.y, q.z, __int_as_float(id));
+  }
+  const_cast<float4*>(a.pts)[j] = p;
 }
 
 // One warp per global tile: find its view, then queue the tile's items.
@@ -1374,11 +1423,11 @@ int32_t sampling_grid(int* blocks, int* sm_count = nullptr) {
 static constexpr size_t align256s(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct SchedLayout {
-  size_t work, item, order, view, small, total;
+  size_t work, item, order, view, small, pts, total;
 };
 
 // up to kTileH items per tile (every row its own item)
-static SchedLayout sched_layout(int64_t H, int64_t W) {
+static SchedLayout sched_layout(int64_t H, int64_t W, int64_t n_sorted) {
   const int64_t ntiles = ((W + kTileW - 1) / kTileW) * ((H + kTileH - 1) / kTileH);
   const size_t per = align256s(sizeof(int) * (size_t)(ntiles * kTileH));
   SchedLayout L;
@@ -1387,7 +1436,8 @@ static SchedLayout sched_layout(int64_t H, int64_t W) {
   L.order = 2 * per;
   L.view = 0;  // single view: none
   L.small = 3 * per;
-  L.total = L.small + 512;  // counts[32], fill[32], next, n_items
+  L.pts = L.small + 512;  // counts[32], fill[32], next, n_items
+  L.total = L.pts + align256s(sizeof(float4) * (size_t)n_sorted);
   return L;
 }
 
@@ -1395,10 +1445,10 @@ static SchedLayout sched_layout(int64_t H, int64_t W) {
 // arguments, the views' first tiles and room for a copy of the view table.
 struct BatchLayout {
   SchedLayout q;
-  size_t args, tile_base, views, buckets, total;
+  size_t args, tile_base, pack_base, views, buckets, pts, total;
 };
 
-static BatchLayout batch_layout(int64_t total_tiles, int n_views) {
+static BatchLayout batch_layout(int64_t total_tiles, int n_views, int64_t total_slots) {
   BatchLayout B;
   const size_t per = align256s(sizeof(int) * (size_t)(total_tiles * kTileH));
   B.q.work = 0;
@@ -1409,9 +1459,11 @@ static BatchLayout batch_layout(int64_t total_tiles, int n_views) {
   B.q.total = B.q.small + 512;  // next, n_items (counts and fill live in `buckets`)
   B.args = B.q.total;
   B.tile_base = B.args + align256s(sizeof(SampleArgs) * (size_t)n_views);
-  B.views = B.tile_base + align256s(sizeof(int) * (size_t)(n_views + 1));
+  B.pack_base = B.tile_base + align256s(sizeof(int) * (size_t)(n_views + 1));
+  B.views = B.pack_base + align256s(sizeof(int) * (size_t)(n_views + 1));
   B.buckets = B.views + align256s(sizeof(hp_view) * (size_t)n_views);  // counts, fill, base: n_views * 32 each
-  B.total = B.buckets + 3 * align256s(sizeof(int) * 32 * (size_t)n_views);
+  B.pts = B.buckets + 3 * align256s(sizeof(int) * 32 * (size_t)n_views);
+  B.total = B.pts + sizeof(float4) * (size_t)total_slots;
   return B;
 }
 
@@ -1452,9 +1504,9 @@ DevOptions dev_options(const hp_options* o) {
 
 using namespace hp;
 
-extern "C" size_t hp_quick_sampling_workspace_size(int32_t height, int32_t width) {
-  if (height <= 0 || width <= 0) return 0;
-  return sched_layout(height, width).total;
+extern "C" size_t hp_quick_sampling_workspace_size(int64_t n_sorted, int32_t height, int32_t width) {
+  if (height <= 0 || width <= 0 || n_sorted < 0) return 0;
+  return sched_layout(height, width, n_sorted).total;
 }
 
 // Argument checks shared by the per-view and batched entry points.
@@ -1492,13 +1544,14 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   if (int32_t rc = check_sampling("hp_quick_sampling", xyz, n_points, cam, opt, sorted_point_idx, n_sorted, hash_table,
                                   sp_xyz, pc_idx, sp_t, mask))
     return rc;
-  const SchedLayout L = sched_layout(cam->height, cam->width);
+  const SchedLayout L = sched_layout(cam->height, cam->width, n_sorted);
   if (!workspace || workspace_bytes < L.total || ((uintptr_t)workspace & 255) != 0)
     return set_error(HP_ERR_WORKSPACE, "hp_quick_sampling: workspace needs %zu bytes, 256-byte aligned (got %zu)",
                      L.total, workspace_bytes);
   SampleArgs a;
   a.xyz = xyz;
   a.sidx = sorted_point_idx;
+  a.pts = (const float4*)((char*)workspace + L.pts);
   a.hash = (const int2*)hash_table;
   a.n_points = (int)n_points;
   a.n_sorted = (int)n_sorted;
@@ -1526,6 +1579,11 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   cudaStream_t st = (cudaStream_t)stream;
   if (cudaMemsetAsync(sc.counts, 0, 512, st) != cudaSuccess)
     return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaMemsetAsync failed");
+  if (n_sorted > 0) {
+    k_pack_points<<<(unsigned)((n_sorted + 255) / 256), 256, 0, st>>>(sorted_point_idx, (int)n_sorted, xyz,
+                                                                      (int)n_points, (float4*)(ws + L.pts));
+    if (int32_t rc = check_launch("k_pack_points")) return rc;
+  }
   k_tile_work<<<(ntiles + 7) / 8, 256, 0, st>>>(a.hash, a.n_sorted, cam->height, cam->width, opt->kernel_size, tiles_x,
                                                  ntiles, sc);
   if (int32_t rc = check_launch("k_tile_work")) return rc;
@@ -1533,6 +1591,13 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   if (int32_t rc = check_launch("k_tile_order")) return rc;
   k_quick_sampling<<<blocks < ntiles ? blocks : ntiles, kThreads, sizeof(Stage), st>>>(a, sc, tiles_x);
   return check_launch("k_quick_sampling");
+}
+
+// packed-point slots of a batch: each view's n_sorted rounded up to 16
+static int64_t batch_slots(const hp_view* views, int32_t n_views) {
+  int64_t total = 0;
+  for (int32_t v = 0; v < n_views; v++) total += (views[v].n_sorted + 15) & ~(int64_t)15;
+  return total;
 }
 
 static int64_t batch_tiles(const hp_view* views, int32_t n_views) {
@@ -1545,8 +1610,8 @@ static int64_t batch_tiles(const hp_view* views, int32_t n_views) {
 extern "C" size_t hp_quick_sampling_batch_workspace_size(const hp_view* views, int32_t n_views) {
   if (!views || n_views <= 0) return 0;
   for (int32_t v = 0; v < n_views; v++)
-    if (views[v].cam.width <= 0 || views[v].cam.height <= 0) return 0;
-  return batch_layout(batch_tiles(views, n_views), n_views).total;
+    if (views[v].cam.width <= 0 || views[v].cam.height <= 0 || views[v].n_sorted < 0) return 0;
+  return batch_layout(batch_tiles(views, n_views), n_views, batch_slots(views, n_views)).total;
 }
 
 extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* views_device, int32_t n_views,
@@ -1572,8 +1637,10 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
     }
   }
   const int64_t total_tiles = batch_tiles(views, n_views);
-  if (total_tiles * kTileH >= (1ll << 31)) return set_error(HP_ERR_INVALID_ARGUMENT, "%s: too many tiles", who);
-  const BatchLayout B = batch_layout(total_tiles, n_views);
+  const int64_t total_slots = batch_slots(views, n_views);
+  if (total_tiles * kTileH >= (1ll << 31) || total_slots >= (1ll << 31))
+    return set_error(HP_ERR_INVALID_ARGUMENT, "%s: too many tiles or points in one batch", who);
+  const BatchLayout B = batch_layout(total_tiles, n_views, total_slots);
   if (!workspace || workspace_bytes < B.total || ((uintptr_t)workspace & 255) != 0)
     return set_error(HP_ERR_WORKSPACE, "%s: workspace needs %zu bytes, 256-byte aligned (got %zu)", who, B.total,
                      workspace_bytes);
@@ -1604,8 +1671,13 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
   if (cudaMemsetAsync(ws + B.q.small, 0, 512, st) != cudaSuccess ||
       cudaMemsetAsync(ws + B.buckets, 0, 2 * bucket_bytes, st) != cudaSuccess)
     return set_error(HP_ERR_CUDA, "%s: memset failed", who);
-  k_batch_setup<<<1, 32, 0, st>>>(views_device, n_views, heavy, args, tile_base);
+  int* pack_base = (int*)(ws + B.pack_base);
+  k_batch_setup<<<1, 32, 0, st>>>(views_device, n_views, heavy, args, tile_base, pack_base, (float4*)(ws + B.pts));
   if (int32_t rc = check_launch("k_batch_setup")) return rc;
+  if (total_slots > 0) {
+    k_batch_pack<<<(unsigned)((total_slots + 255) / 256), 256, 0, st>>>(args, pack_base, n_views, (int)total_slots);
+    if (int32_t rc = check_launch("k_batch_pack")) return rc;
+  }
   const int nt = (int)total_tiles;
   k_batch_tile_work<<<(nt + 7) / 8, 256, 0, st>>>(args, tile_base, n_views, nt, sc);
   if (int32_t rc = check_launch("k_batch_tile_work")) return rc;

@@ -130,7 +130,7 @@ class BatchRenderer:
         L = native.lib()
         st = _vp(torch.cuda.current_stream(self.device).cuda_stream)
         if getattr(self, "_pv_ws", None) is None:
-            need = max(L.hp_quick_sampling_workspace_size(v.H, v.W) for v in self.views)
+            need = max(L.hp_quick_sampling_workspace_size(v.n, v.H, v.W) for v in self.views)
             self._pv_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
             self._pv_opt = ops.make_options(self.options)
         ws = self._pv_ws

@@ -59,7 +59,7 @@ class ViewPipeline:
         self.pc_idx = torch.empty((self.H, self.W, S, P), dtype=torch.int32, device=dev)
         self.sp_t = torch.empty((self.H, self.W, S), dtype=torch.float32, device=dev)
         self.mask = torch.empty((self.H, self.W, S), dtype=torch.bool, device=dev)
-        self.ws_sample_bytes = L.hp_quick_sampling_workspace_size(self.H, self.W)
+        self.ws_sample_bytes = L.hp_quick_sampling_workspace_size(self.n, self.H, self.W)
         self.ws_sample = torch.empty(self.ws_sample_bytes, dtype=torch.uint8, device=dev)
 
     def build(self, xyz, cam, stream):

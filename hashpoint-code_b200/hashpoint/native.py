@@ -153,7 +153,7 @@ def lib():
         L.hp_pts2plane_noalloc.restype = i32
         L.hp_scatter_hashtable.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp, vp]
         L.hp_scatter_hashtable.restype = i32
-        L.hp_quick_sampling_workspace_size.argtypes = [i32, i32]
+        L.hp_quick_sampling_workspace_size.argtypes = [i64, i32, i32]
         L.hp_quick_sampling_workspace_size.restype = sz
         L.hp_quick_sampling.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, vp, vp, vp, vp, sz, vp]
         L.hp_quick_sampling.restype = i32

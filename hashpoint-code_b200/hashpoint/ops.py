@@ -135,7 +135,7 @@ def quick_sampling(xyz, c2w, fx, fy, cx, cy, width, height, opt, sorted_point_id
     cam = make_camera(c2w=c2w, fx=fx, fy=fy, cx=cx, cy=cy, width=W, height=H)
     o = make_options(opt)
     L = native.lib()
-    ws_bytes = L.hp_quick_sampling_workspace_size(H, W)
+    ws_bytes = L.hp_quick_sampling_workspace_size(sorted_point_idx.numel(), H, W)
     ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
     rc = L.hp_quick_sampling(_ptr(xyz), xyz.shape[0], ctypes.byref(cam), ctypes.byref(o), _ptr(sorted_point_idx),
                              sorted_point_idx.numel(), _ptr(hash_table), _ptr(sp_xyz), _ptr(pc_idx), _ptr(sp_t),

@@ -192,9 +192,10 @@ HP_API int32_t hp_render(const float* deltas, const float* t_val, float vsize, c
                          const float* rgbs, int64_t n_rays, int32_t S, int32_t white_bg, float* color,
                          hp_stream_t stream);
 
-/* Scratch bytes hp_quick_sampling needs for an image of this size (its tile
- * schedule); workspace must be 256-byte aligned. */
-HP_API size_t hp_quick_sampling_workspace_size(int32_t height, int32_t width);
+/* Scratch bytes hp_quick_sampling needs for n_sorted ids and an image of this
+ * size (its tile schedule and the ids' points packed as 16-byte records);
+ * workspace must be 256-byte aligned. */
+HP_API size_t hp_quick_sampling_workspace_size(int64_t n_sorted, int32_t height, int32_t width);
 
 /* Launch tuning of hp_quick_sampling_batch (NULL or 0 fields = defaults).
  * Outputs never depend on it.  heavy_window: rays whose window holds more

@@ -110,7 +110,7 @@ def test_quick_sampling_rejects_null_and_misaligned(L):
                                None) == -1
     assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, -1, p, p, p, p, p, ws, big,
                                None) == -1
-    need = L.hp_quick_sampling_workspace_size(8, 8)
+    need = L.hp_quick_sampling_workspace_size(10, 8, 8)
     assert need > 0
     assert L.hp_quick_sampling(p, 10, ctypes.byref(_cam()), ctypes.byref(_opt()), p, 10, p, p, p, p, p, ws, need - 1,
                                None) == -2
