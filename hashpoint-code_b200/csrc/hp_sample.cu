@@ -855,6 +855,7 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
     float ts[kBallPass], reach[kBallPass], spx[kBallPass], spy[kBallPass], spz[kBallPass], maxd[kBallPass];
     float bd[kBallPass][kBallBuf];
     int bi[kBallPass][kBallBuf], bsize[kBallPass], maxi[kBallPass];
+    bool settled[kBallPass];
 #pragma unroll
     for (int q = 0; q < kBallPass; q++) {
       float t = 0.0f;
@@ -872,6 +873,7 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
       bsize[q] = 0;
       maxi[q] = 0;
       maxd[q] = 1e3f;
+      settled[q] = false;
 #pragma unroll
       for (int e = 0; e < kBallBuf; e++) bd[q][e] = 0.0f, bi[q][e] = -1;
     }
@@ -896,7 +898,9 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
       }
 #pragma unroll
       for (int q = 0; q < kBallPass; q++) {
-        unsigned mm = __ballot_sync(kAll, hq[q]);
+        // once the buffer is full and has had a replacement, maxd is its true
+        // maximum and only decreases, so hits at or beyond it cannot change it
+        unsigned mm = __ballot_sync(kAll, hq[q] && (!settled[q] || dq[q] < maxd[q]));
         while (mm) {
           const int l = __ffs(mm) - 1;
           mm &= mm - 1;
@@ -925,6 +929,7 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
               }
             maxd[q] = md;
             maxi[q] = mi;
+            settled[q] = true;
           }
         }
       }
