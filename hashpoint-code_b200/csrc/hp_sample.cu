@@ -58,6 +58,7 @@ constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
 constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
 constexpr int kStageCap = 3584;  // staged points per tile (56 KB)
 constexpr int kSplitWork = kStageCap;  // tiles whose halo holds more points are split into row bands
+constexpr int kItemsPerTile = kTileH * 4;  // rows, each in up to four column quarters
 #ifndef HP_BIN_LIST
 #define HP_BIN_LIST 6
 #endif
@@ -960,7 +961,10 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
 // and is very uneven (dense objects vs background).  Work items are tiles of
 // 8 rows x 32 pixels; a tile whose halo does not fit the stage is split into
 // items of 4, 2 or 1 rows (each staged on its own, so they run concurrently
-// on different SMs).  Items are handed out heaviest first (a counting sort on
+// on different SMs), and a single row whose halo still does not fit into
+// column halves and then quarters, each staging its own, narrower halo; only
+// what does not fit even then reads candidates from global memory.  Items are
+// handed out heaviest first (a counting sort on
 // log2 of the halo's point count; halos still too large to stage weighted up)
 // to a persistent grid of SMs x resident blocks that takes the next item from
 // an atomic counter, so heavy items start first and light ones fill in
@@ -968,6 +972,7 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
 struct Sched {
   int* work;    // [max items] estimated cost
   int* item;    // [max items] (tile << 8) | (first row << 4) | rows
+  int* cols;    // [max items] (first column << 8) | end column, within the tile
   int* view;    // [max items] view of the item (batched launches; else null)
   int* order;   // [max items] item indices, heaviest first
   int* counts;  // [32] items per cost class
@@ -978,12 +983,12 @@ struct Sched {
 
 __device__ __forceinline__ int cost_class(int w) { return 31 - __clz(w | 1); }
 
-// Points in the window halo of rows [vb, vb + rows) of a tile's columns (one warp).
+// Points in the window halo of rows [vb, vb + rows) and tile columns [c0, c1) (one warp).
 __device__ __forceinline__ int halo_points(const int2* __restrict__ hash, int n_sorted, int H, int W, int k, int vb,
-                                           int rows, int u0) {
+                                           int rows, int u0, int c0 = 0, int c1 = kTileW) {
   const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
   const int rv0 = max(0, vb - lo), rv1 = min(H - 1, vb + rows - 1 + hi);
-  const int ru0 = max(0, u0 - lo), ru1 = min(W - 1, u0 + kTileW - 1 + hi);
+  const int ru0 = max(0, u0 + c0 - lo), ru1 = min(W - 1, u0 + c1 - 1 + hi);
   const int nu = ru1 - ru0 + 1, ncells = (rv1 - rv0 + 1) * nu;
   int sum = 0;
   for (int c = (threadIdx.x & 31); c < ncells; c += 32) {
@@ -1010,16 +1015,33 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
       rows = (rows + 1) >> 1;
       sum = halo_points(hash, n_sorted, H, W, k, vb, rows, u0);
     }
-    if (lane == 0) {
-      // cost estimate: the halo's points scaled by the share of its rows that
-      // hold the item's rays; unstaged items (global memory reads) count 4x
-      const int c = (int)(((long long)min(sum, 1 << 24) * rows * kTileH) / (rows + k - 1));
-      const int w = sum > kStageCap ? c * 4 : c;
-      const int i = atomicAdd(sc.n_items, 1);
-      sc.work[i] = w;
-      sc.item[i] = (t << 8) | ((vb - v0) << 4) | rows;
-      if (sc.view) sc.view[i] = view;
-      atomicAdd(sc.counts + (sc.view ? view * 32 : 0) + cost_class(w), 1);
+    // cost estimate: the halo's points scaled by the share of its rows (and
+    // columns) that hold the item's rays; unstaged items count 4x
+    auto emit = [&](int hs, int c0, int c1) {
+      if (lane == 0) {
+        const int c = (int)(((long long)min(hs, 1 << 24) * rows * kTileH * (c1 - c0)) /
+                            ((long long)(rows + k - 1) * (c1 - c0 + k - 1)));
+        const int w = hs > kStageCap ? c * 4 : c;
+        const int i = atomicAdd(sc.n_items, 1);
+        sc.work[i] = w;
+        sc.item[i] = (t << 8) | ((vb - v0) << 4) | rows;
+        sc.cols[i] = (c0 << 8) | c1;
+        if (sc.view) sc.view[i] = view;
+        atomicAdd(sc.counts + (sc.view ? view * 32 : 0) + cost_class(w), 1);
+      }
+    };
+    if (sum <= kStageCap) {
+      emit(sum, 0, kTileW);
+    } else {  // one row: halves, then quarters, until the halo fits
+      for (int c0 = 0; c0 < kTileW && u0 + c0 < W; c0 += kTileW / 2) {
+        const int hs = halo_points(hash, n_sorted, H, W, k, vb, rows, u0, c0, c0 + kTileW / 2);
+        if (hs <= kStageCap) {
+          emit(hs, c0, c0 + kTileW / 2);
+          continue;
+        }
+        for (int q0 = c0; q0 < c0 + kTileW / 2 && u0 + q0 < W; q0 += kTileW / 4)
+          emit(halo_points(hash, n_sorted, H, W, k, vb, rows, u0, q0, q0 + kTileW / 4), q0, q0 + kTileW / 4);
+      }
     }
     vb += rows;
   }
@@ -1087,11 +1109,14 @@ __global__ void __launch_bounds__(256) k_batch_order_place(Sched sc, const int* 
   }
 }
 
-__device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int v0, int rows, int u0) {
+// Rays of rows [v0, v0 + rows) and tile columns [c0, c1) of the tile at u0
+// (u0 + c0 < width).
+__device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int v0, int rows, int u0, int c0 = 0,
+                                             int c1 = kTileW) {
   const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
   const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
   const int rv0 = max(0, v0 - lo), rv1 = min(H - 1, v0 + rows - 1 + hi);
-  const int ru0 = max(0, u0 - lo), ru1 = min(W - 1, u0 + kTileW - 1 + hi);
+  const int ru0 = max(0, u0 + c0 - lo), ru1 = min(W - 1, u0 + c1 - 1 + hi);
   const int nu = ru1 - ru0 + 1, ncells = (rv1 - rv0 + 1) * nu;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
@@ -1161,7 +1186,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
   {
     const int pu = u0 + (tid & 31), pv = v0 + (tid >> 5);
     int T = -1;  // window candidates; -1: no ray at this pixel
-    if (pu < W && pv < H && (tid >> 5) < rows) {
+    if (pu < W && pv < H && (tid >> 5) < rows && (tid & 31) >= c0 && (tid & 31) < c1) {
       T = 0;
       if (staged && pu - lo >= 0 && pu + hi <= W - 1) {
         // unclamped columns: each window row is a run of k consecutive halo cells
@@ -1240,9 +1265,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a, Sc
     __syncthreads();
     const int i = s_next;
     if (i >= n) break;
-    const int it = sc.item[sc.order[i]];
+    const int j = sc.order[i];
+    const int it = sc.item[j], cc = sc.cols[j];
     const int t = it >> 8;
-    process_tile(a, st, (t / tiles_x) * kTileH + ((it >> 4) & 15), it & 15, (t % tiles_x) * kTileW);
+    process_tile(a, st, (t / tiles_x) * kTileH + ((it >> 4) & 15), it & 15, (t % tiles_x) * kTileW, cc >> 8,
+                 cc & 255);
   }
 }
 
@@ -1381,10 +1408,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_quick_sampling_batch(const Samp
     const int j = sc.order[i];
     if (threadIdx.x == 0) s_args = args[sc.view[j]];
     __syncthreads();
-    const int it = sc.item[j];
+    const int it = sc.item[j], cc = sc.cols[j];
     const int t = it >> 8;
     const int tiles_x = (s_args.cam.width + kTileW - 1) / kTileW;
-    process_tile(s_args, st, (t / tiles_x) * kTileH + ((it >> 4) & 15), it & 15, (t % tiles_x) * kTileW);
+    process_tile(s_args, st, (t / tiles_x) * kTileH + ((it >> 4) & 15), it & 15, (t % tiles_x) * kTileW, cc >> 8,
+                 cc & 255);
   }
 }
 
@@ -1428,19 +1456,20 @@ int32_t sampling_grid(int* blocks, int* sm_count = nullptr) {
 static constexpr size_t align256s(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct SchedLayout {
-  size_t work, item, order, view, small, pts, total;
+  size_t work, item, cols, order, view, small, pts, total;
 };
 
-// up to kTileH items per tile (every row its own item)
+// up to kItemsPerTile items per tile (every row its own item, in quarters)
 static SchedLayout sched_layout(int64_t H, int64_t W, int64_t n_sorted) {
   const int64_t ntiles = ((W + kTileW - 1) / kTileW) * ((H + kTileH - 1) / kTileH);
-  const size_t per = align256s(sizeof(int) * (size_t)(ntiles * kTileH));
+  const size_t per = align256s(sizeof(int) * (size_t)(ntiles * kItemsPerTile));
   SchedLayout L;
   L.work = 0;
   L.item = per;
-  L.order = 2 * per;
+  L.cols = 2 * per;
+  L.order = 3 * per;
   L.view = 0;  // single view: none
-  L.small = 3 * per;
+  L.small = 4 * per;
   L.pts = L.small + 512;  // counts[32], fill[32], next, n_items
   L.total = L.pts + align256s(sizeof(float4) * (size_t)n_sorted);
   return L;
@@ -1455,12 +1484,13 @@ struct BatchLayout {
 
 static BatchLayout batch_layout(int64_t total_tiles, int n_views, int64_t total_slots) {
   BatchLayout B;
-  const size_t per = align256s(sizeof(int) * (size_t)(total_tiles * kTileH));
+  const size_t per = align256s(sizeof(int) * (size_t)(total_tiles * kItemsPerTile));
   B.q.work = 0;
   B.q.item = per;
-  B.q.order = 2 * per;
-  B.q.view = 3 * per;
-  B.q.small = 4 * per;
+  B.q.cols = 2 * per;
+  B.q.order = 3 * per;
+  B.q.view = 4 * per;
+  B.q.small = 5 * per;
   B.q.total = B.q.small + 512;  // next, n_items (counts and fill live in `buckets`)
   B.args = B.q.total;
   B.tile_base = B.args + align256s(sizeof(SampleArgs) * (size_t)n_views);
@@ -1575,6 +1605,7 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   Sched sc;
   sc.work = (int*)(ws + L.work);
   sc.item = (int*)(ws + L.item);
+  sc.cols = (int*)(ws + L.cols);
   sc.order = (int*)(ws + L.order);
   sc.view = nullptr;
   sc.counts = (int*)(ws + L.small);
@@ -1643,7 +1674,7 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
   }
   const int64_t total_tiles = batch_tiles(views, n_views);
   const int64_t total_slots = batch_slots(views, n_views);
-  if (total_tiles * kTileH >= (1ll << 31) || total_slots >= (1ll << 31))
+  if (total_tiles * kItemsPerTile >= (1ll << 31) || total_slots >= (1ll << 31))
     return set_error(HP_ERR_INVALID_ARGUMENT, "%s: too many tiles or points in one batch", who);
   const BatchLayout B = batch_layout(total_tiles, n_views, total_slots);
   if (!workspace || workspace_bytes < B.total || ((uintptr_t)workspace & 255) != 0)
@@ -1663,6 +1694,7 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
   Sched sc;
   sc.work = (int*)(ws + B.q.work);
   sc.item = (int*)(ws + B.q.item);
+  sc.cols = (int*)(ws + B.q.cols);
   sc.order = (int*)(ws + B.q.order);
   sc.view = (int*)(ws + B.q.view);
   const size_t bucket_bytes = align256s(sizeof(int) * 32 * (size_t)n_views);
