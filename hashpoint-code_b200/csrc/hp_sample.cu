@@ -677,6 +677,27 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
       body(j0, j < total, idx, c, pc);
     }
   };
+  // The same for the capped passes (A, B and the walk sums; carry = the
+  // pass's per-cell kept counts): when the cell the chunk ended in already
+  // has its 48 kept candidates, the rest of it is skipped -- none of them can
+  // be kept.
+  auto capped_chunks = [&](const int& carry, auto&& body) {
+    for (int j0 = 0; j0 < total;) {
+      const int j = j0 + lane;
+      int c = 0;
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1)
+        if (__shfl_sync(kAll, cpre, c + s) <= j) c += s;
+      const int pc = __shfl_sync(kAll, cpre, c);
+      const int idx = __shfl_sync(kAll, cbase, c) + (j - pc);
+      body(j0, j < total, idx, c, pc);
+      j0 += 32;
+      if (capped) {
+        const int last = __shfl_sync(kAll, c, 31);
+        if (__shfl_sync(kAll, carry, last) >= kKeptPerCell) j0 = max(j0, __shfl_sync(kAll, cpre + ccnt, last));
+      }
+    }
+  };
   // the candidate's t and offset from the ray; true when within the radius
   auto eval = [&](bool valid, int idx, float& t, float& e0, float& e1, float& e2) -> bool {
     if (!valid) return false;
@@ -707,7 +728,7 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
   float tmin = 1e3f, tmax = -1e3f;
   {
     int carry = 0;
-    chunks([&](int j0, bool valid, int idx, int cell, int pc) {
+    capped_chunks(carry, [&](int j0, bool valid, int idx, int cell, int pc) {
       float t = 0.f, e0, e1, e2;
       if (accept(eval(valid, idx, t, e0, e1, e2), j0, cell, pc, carry)) {
         if (tmin > t) tmin = t;
@@ -738,7 +759,7 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
     for (int q = 0; q < kBins / 32; q++) s1[q] = 0u, s2[q] = 0u;
     {
       int carry = 0;
-      chunks([&](int j0, bool valid, int idx, int cell, int pc) {
+      capped_chunks(carry, [&](int j0, bool valid, int idx, int cell, int pc) {
         float t = 0.f, e0, e1, e2;
         if (accept(eval(valid, idx, t, e0, e1, e2), j0, cell, pc, carry)) {
           const int b = bin_of(t, tmin);
@@ -795,7 +816,7 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
 #pragma unroll
       for (int q = 0; q < kWalkBatch; q++) bsum[q] = 0.0f, bcnt[q] = 0;
       int carry = 0;
-      chunks([&](int j0, bool valid, int idx, int cell, int pc) {
+      capped_chunks(carry, [&](int j0, bool valid, int idx, int cell, int pc) {
         float t = 0.f, e0 = 0.f, e1 = 0.f, e2 = 0.f;
         int mine = -1;
         float dist = 0.0f;
