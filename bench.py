@@ -164,7 +164,12 @@ def run_gpu(args):
     dev = torch.device("cuda", local)
     native.build()
 
+    from hashpoint import shard
     sc = synth.make_shapes(n_views=args.views, seed=0, with_feat=True)
+    if rank > 0:  # the same cloud, this rank's own cameras
+        cams = synth.orbit_cameras(np.random.default_rng(shard.view_seed(0, rank)), args.views, 4.0, 800, 800, 1111.0,
+                                   400.0, 400.0)
+        sc.cameras[:] = cams
     xyz = torch.from_numpy(sc.xyz).to(dev)
     feat = torch.from_numpy(sc.feat).to(dev)  # resident, never read by the path
     cams = CameraTable(sc.cameras, dev)
@@ -226,13 +231,7 @@ def run_gpu(args):
     t_wall = time.perf_counter() - t_wall0
     clk = clocks.stop()
 
-    ms_per_step = sum(step_ms) / len(step_ms)
-    if world > 1:
-        t = torch.tensor([ms_per_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_per_step = float(t.item())
-    rays_per_step = HW * len(structs) * world
-    value = rays_per_step / (ms_per_step * 1e-3)
+    value, ms_per_step = shard.job_rays_per_s(HW * len(structs), sum(step_ms) / len(step_ms), dev)
 
     # roofline of the dominant kernel (k_quick_sampling)
     peaks = {}
@@ -255,9 +254,10 @@ def run_gpu(args):
     e2e = run_e2e(args, sc, dev, pipe_hw=HW)
 
     # the two system forms beside the plain per-view launch (one GPU runs them alone)
-    batched = served = downstream = None
+    batched = served = downstream = others = None
     if world == 1 and not args.no_systems:
         downstream = run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
+        others = run_other_configs(dev, flush)
         del pipe
         torch.cuda.empty_cache()
         batched = run_batched(args, dev, xyz, sc, flush)
@@ -282,6 +282,8 @@ def run_gpu(args):
     }
     if downstream is not None:
         result["downstream"] = downstream
+    if others is not None:
+        result["other_configs"] = others
     if batched is not None:
         result["batched"] = batched
     if served is not None:
@@ -416,6 +418,41 @@ def run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
             "render": {"ms_per_view": rr, "bytes_per_view": rb, "gbs": rb / (rr * 1e-3) / 1e9,
                        "frac_of_hbm": rb / (rr * 1e-3) / 1e9 / peak, "note": "clamp_t fused"},
             "views": len(fq_ms)}
+
+
+def run_other_configs(dev, flush):
+    """Configs 1 and 3 through the same plain per-view launch (CUDA events, L2 flushed):
+    the 100k-point sphere at 400x400 (k=3) and the 3M-point clusters at 1600x1200 (K=16)."""
+    import torch
+
+    from hashpoint import synth
+    from hashpoint.engine import CameraTable, ViewPipeline
+
+    out = {}
+    for name, sc in (("sphere_100k_400x400", synth.make_sphere()), ("clusters_3M_1600x1200", synth.make_clusters(n_views=4))):
+        X = torch.from_numpy(sc.xyz).to(dev)
+        c0 = sc.cameras[0]
+        pipe = ViewPipeline(len(sc.xyz), c0.height, c0.width, sc.options, dev)
+        cams = CameraTable(sc.cameras, dev)
+        structs = [cams.struct(i) for i in range(cams.n)]
+        for s_ in structs:
+            pipe.render(X, s_)
+        ts = []
+        for _ in range(3):
+            for s_ in structs:
+                flush.fill_(1)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                pipe.render(X, s_)
+                e1.record()
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+        ms = statistics.median(ts)
+        out[name] = {"rays_per_s": c0.width * c0.height / (ms * 1e-3), "ms_per_view": ms, "views": len(structs),
+                     "points": len(sc.xyz)}
+        del pipe, X
+        torch.cuda.empty_cache()
+    return out
 
 
 def run_batched(args, dev, xyz, sc, flush):
