@@ -1646,7 +1646,9 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   if (int32_t rc = check_launch("k_tile_work")) return rc;
   k_tile_order<<<(ntiles + 255) / 256 < 148 ? (ntiles + 255) / 256 : 148, 256, 0, st>>>(sc);
   if (int32_t rc = check_launch("k_tile_order")) return rc;
-  k_quick_sampling<<<blocks < ntiles ? blocks : ntiles, kThreads, sizeof(Stage), st>>>(a, sc, tiles_x);
+  // a split tile yields up to kItemsPerTile items: size the persistent grid by those, not by tiles
+  const int64_t max_items = (int64_t)ntiles * kItemsPerTile;
+  k_quick_sampling<<<blocks < max_items ? blocks : (int)max_items, kThreads, sizeof(Stage), st>>>(a, sc, tiles_x);
   return check_launch("k_quick_sampling");
 }
 
@@ -1743,7 +1745,8 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
   if (int32_t rc = check_launch("k_batch_order_scan")) return rc;
   k_batch_order_place<<<(nt + 255) / 256 < 148 ? (nt + 255) / 256 : 148, 256, 0, st>>>(sc, base);
   if (int32_t rc = check_launch("k_batch_order_place")) return rc;
-  k_quick_sampling_batch<<<blocks < nt ? blocks : nt, kThreads, sizeof(Stage), st>>>(args, sc);
+  const int64_t max_items = (int64_t)nt * kItemsPerTile;
+  k_quick_sampling_batch<<<blocks < max_items ? blocks : (int)max_items, kThreads, sizeof(Stage), st>>>(args, sc);
   return check_launch("k_quick_sampling_batch");
 }
 
