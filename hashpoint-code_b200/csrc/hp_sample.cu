@@ -56,7 +56,8 @@ constexpr int kTileH = 8;    // rows per block
 constexpr int kThreads = kTileW * kTileH;
 constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
 constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
-constexpr int kStageCap = 3584;  // staged points per tile (56 KB)
+constexpr int kStageCap = 2560;  // staged points per tile (40 KB)
+constexpr int kBlocksPerSM = 4;  // resident sampling blocks per SM (64 registers, 57 KB shared memory each)
 constexpr int kSplitWork = kStageCap;  // tiles whose halo holds more points are split into row bands
 constexpr int kItemsPerTile = kTileH * 4;  // rows, each in up to four column quarters
 #ifndef HP_BIN_LIST
@@ -98,8 +99,8 @@ struct Stage {
   int next_unit;            // next work unit of the tile (see process_tile)
   unsigned kept[kMaskWords][kThreads];  // per thread: window positions pass A accepted
 };
-// three CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
-static_assert(3 * (sizeof(Stage) + 16 + 1024) <= 228 * 1024, "stage too large for three CTAs per SM");
+// kBlocksPerSM CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
+static_assert(kBlocksPerSM * (sizeof(Stage) + 16 + 1024) <= 228 * 1024, "stage too large for the blocks per SM");
 
 // Clipped bucket range of a hash entry: [x, x + count) within [0, n_sorted).
 __device__ __forceinline__ int2 bucket_range(int2 h, int n_sorted) {
@@ -1276,7 +1277,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
   __syncthreads();  // the stage is reused by the next tile
 }
 
-__global__ void __launch_bounds__(kThreads, 3) k_quick_sampling(SampleArgs a, Sched sc, int tiles_x) {
+__global__ void __launch_bounds__(kThreads, kBlocksPerSM) k_quick_sampling(SampleArgs a, Sched sc, int tiles_x) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Stage& st = *reinterpret_cast<Stage*>(smem_raw);
   __shared__ int s_next;
@@ -1415,7 +1416,7 @@ __global__ void __launch_bounds__(256) k_batch_tile_work(const SampleArgs* __res
 
 // The persistent sampling kernel over the batch's queue; each item's view
 // arguments are loaded into shared memory before the tile is processed.
-__global__ void __launch_bounds__(kThreads, 3) k_quick_sampling_batch(const SampleArgs* __restrict__ args, Sched sc) {
+__global__ void __launch_bounds__(kThreads, kBlocksPerSM) k_quick_sampling_batch(const SampleArgs* __restrict__ args, Sched sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Stage& st = *reinterpret_cast<Stage*>(smem_raw);
   __shared__ int s_next;
