@@ -1023,19 +1023,60 @@ __device__ __forceinline__ int halo_points(const int2* __restrict__ hash, int n_
 }
 
 // Items of tile t (local to its view) of an H x W image, appended to the queue.
+// The clipped point counts of the tile's whole window halo (up to 12 rows x
+// 36 columns) are loaded once, two columns per lane; the halo of any row band
+// or column range of the tile is a sub-rectangle of it, summed from those
+// registers with one warp reduction.
 __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k, int tiles_x,
                                           int t, int view, Sched& sc) {
+  constexpr int kHaloRows = kTileH + kMaxKernel - 1;
   const int lane = threadIdx.x & 31;
   const int v0 = (t / tiles_x) * kTileH, u0 = (t % tiles_x) * kTileW;
   const int v_end = min(H, v0 + kTileH);
+  const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
+  const int hv0 = max(0, v0 - lo), hv1 = min(H - 1, v_end - 1 + hi);
+  const int hu0 = max(0, u0 - lo), hu1 = min(W - 1, u0 + kTileW - 1 + hi);
+  const int ua = hu0 + lane, ub = hu0 + 32 + lane;  // this lane's halo columns
+  int ca[kHaloRows], cb[kHaloRows];
+#pragma unroll
+  for (int h = 0; h < kHaloRows; h++) {
+    ca[h] = 0;
+    cb[h] = 0;
+    const int vv = hv0 + h;
+    if (vv <= hv1) {
+      if (ua <= hu1) {
+        const int2 rg = bucket_range(__ldg(hash + (size_t)vv * W + ua), n_sorted);
+        ca[h] = min(rg.y - rg.x, kStageCap + 1);
+      }
+      if (ub <= hu1) {
+        const int2 rg = bucket_range(__ldg(hash + (size_t)vv * W + ub), n_sorted);
+        cb[h] = min(rg.y - rg.x, kStageCap + 1);
+      }
+    }
+  }
+  // points in the halo of rows [vb, vb + rows) and tile columns [c0, c1)
+  auto halo = [&](int vb, int rows, int c0, int c1) {
+    const int r0 = max(0, vb - lo), r1 = min(H - 1, vb + rows - 1 + hi);
+    const int x0 = max(0, u0 + c0 - lo), x1 = min(W - 1, u0 + c1 - 1 + hi);
+    const bool ia = ua >= x0 && ua <= x1, ib = ub >= x0 && ub <= x1;
+    int sum = 0;
+#pragma unroll
+    for (int h = 0; h < kHaloRows; h++) {
+      const int vv = hv0 + h;
+      if (vv >= r0 && vv <= r1) sum += (ia ? ca[h] : 0) + (ib ? cb[h] : 0);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    return sum;
+  };
   // split the tile's rows until each item's halo holds at most kSplitWork
   // points (so no item runs much longer than the average) or is one row
   for (int vb = v0; vb < v_end;) {
     int rows = v_end - vb;
-    int sum = halo_points(hash, n_sorted, H, W, k, vb, rows, u0);
+    int sum = halo(vb, rows, 0, kTileW);
     while (sum > kSplitWork && rows > 1) {
       rows = (rows + 1) >> 1;
-      sum = halo_points(hash, n_sorted, H, W, k, vb, rows, u0);
+      sum = halo(vb, rows, 0, kTileW);
     }
     // cost estimate: the halo's points scaled by the share of its rows (and
     // columns) that hold the item's rays; unstaged items count 4x
@@ -1056,13 +1097,13 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
       emit(sum, 0, kTileW);
     } else {  // one row: halves, then quarters, until the halo fits
       for (int c0 = 0; c0 < kTileW && u0 + c0 < W; c0 += kTileW / 2) {
-        const int hs = halo_points(hash, n_sorted, H, W, k, vb, rows, u0, c0, c0 + kTileW / 2);
+        const int hs = halo(vb, rows, c0, c0 + kTileW / 2);
         if (hs <= kStageCap) {
           emit(hs, c0, c0 + kTileW / 2);
           continue;
         }
         for (int q0 = c0; q0 < c0 + kTileW / 2 && u0 + q0 < W; q0 += kTileW / 4)
-          emit(halo_points(hash, n_sorted, H, W, k, vb, rows, u0, q0, q0 + kTileW / 4), q0, q0 + kTileW / 4);
+          emit(halo(vb, rows, q0, q0 + kTileW / 4), q0, q0 + kTileW / 4);
       }
     }
     vb += rows;
