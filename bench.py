@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-systems", action="store_true", help="skip the batched and served measurements")
     ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--kernels-once", action="store_true",
+                    help="run one view of the workload once through every kernel of the path and exit (for profilers)")
     return ap.parse_args()
 
 
@@ -568,9 +570,53 @@ def run_reference(args):
     }), flush=True)
 
 
+def run_kernels_once(args):
+    """One view of the workload through every kernel once, after one untimed pass: the projection and
+    hash-table build, the per-view sampling launch, a 4-view batched launch, the listed-ray query,
+    ray directions, the FeatureQuery gather (fp16[32] features), clamp_t and render.  Prints no bench
+    line: this is the command the per-kernel profiles are captured on."""
+    import numpy as np
+    import torch
+
+    from hashpoint import batch, native, ops, synth
+
+    native.build()
+    dev = torch.device("cuda", 0)
+    sc = synth.make_shapes(n_views=4, seed=0, with_feat=True)
+    xyz = torch.from_numpy(sc.xyz).to(dev)
+    feat = torch.from_numpy(sc.feat).to(dev)
+    rng = np.random.default_rng(3)
+    n = xyz.shape[0]
+    rgb = torch.from_numpy(rng.random((n, 3), dtype=np.float32)).to(dev)
+    dr = torch.from_numpy(rng.standard_normal((n, 3)).astype(np.float32)).to(dev)
+    cam = sc.cameras[0]
+    c2w, w2c, K = (torch.from_numpy(np.asarray(a, np.float32)).to(dev) for a in (cam.c2w, cam.w2c, cam.K))
+    S = sc.options.num_sample_points_per_ray
+    R = cam.width * cam.height
+    ray_ids = torch.from_numpy(rng.choice(R, 65536, replace=False).astype(np.int32)).to(dev)
+    sig = torch.rand((R, S), device=dev) * 50
+    rgbs = torch.rand((R, S, 3), device=dev)
+    r = batch.BatchRenderer([xyz], [(0, c) for c in sc.cameras], sc.options, dev)
+    for _ in range(2):  # the first pass loads the library and warms up
+        sidx, _, hsh = ops.pts2plane(xyz, w2c, K, cam.height, cam.width)
+        sp_xyz, pc_idx, sp_t, mask = ops.quick_sampling(xyz, c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width,
+                                                        cam.height, sc.options, sidx, hsh)
+        r.run()
+        ops.quick_query(xyz, c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width, cam.height, sc.options, sidx, hsh,
+                        ray_ids)
+        ops.ray_directions(c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width, cam.height)
+        ops.feature_query(xyz, rgb, dr, feat, sp_xyz, pc_idx, mask, c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width)
+        d = ops.clamp_t(sp_t.view(R, S))
+        ops.render(d, sig, rgbs)
+        torch.cuda.synchronize(dev)
+    print("kernels-once: ok", flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.kernels_once:
+        run_kernels_once(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

@@ -11,6 +11,8 @@ signatures for the search+sample path:
         -> sp_xyz f32[H,W,S,3], pc_idx int32[H,W,S,P], sp_t f32[H,W,S], mask bool[H,W,S]
 
   FeatureQuery().forward(neuralpoints, sp_xyz, pc_idx, mask, cam, ray_index_uv) (:328-387)
+  positional_encoding(positions, freqs, ori=False)                (:389-404)
+  Aggregator().forward(pc_xyz, pc_rgb, pc_dir, pc_feat, sp_xyz, valid, mask_out, rays_d) (:406-507)
   clamp_t(t_val, vsize), render(deltas, sigmas, rgbs, white_bg)   (:508-529)
 
 pts2plane runs the projection, the per-pixel counting sort and the bucket
@@ -293,6 +295,83 @@ class FeatureQuery(nn.Module):
                                  output_sp_xyz.contiguous(), pc_idx.contiguous(), mask_out, cam.c2w,
                                  _scalar(cam.fx), _scalar(cam.fy), _scalar(cam.cx), _scalar(cam.cy),
                                  _scalar(cam.width), uv)
+
+
+def positional_encoding(positions, freqs, ori=False):
+    """sin / cos of every channel times 2^f, f < freqs (epcq.py:389-404): interleaved per argument
+    ([sin a0, cos a0, sin a1, ...], argument c * freqs + f) or, with ori, [positions, all sines,
+    all cosines]."""
+    bands = 2.0 ** torch.arange(freqs, dtype=torch.float32, device=positions.device)
+    args = (positions[..., None] * bands).flatten(-2)
+    if ori:
+        return torch.cat([positions, torch.sin(args), torch.cos(args)], dim=-1)
+    return torch.stack([torch.sin(args), torch.cos(args)], dim=-1).flatten(-2)
+
+
+class Aggregator(nn.Module):
+    """The per-point MLP, alpha branch, inverse-distance aggregation and colour branch (epcq.py:406-507).
+
+    Same layers, names, initialisation and forward signature as the reference's module, so its
+    state_dict loads unchanged.  forward runs on the tensor cores: the weights are packed to bf16
+    operand tiles once per parameter change, and two fused kernels compute the whole forward
+    (bf16 operands, fp32 accumulation; outputs within about 1e-3 of the fp32 reference).  It is
+    an inference path: with autograd recording and parameters that require grad it raises."""
+
+    def __init__(self) -> None:
+        super().__init__()
+
+        def act():
+            return nn.LeakyReLU(inplace=True)
+
+        self.block1 = nn.Sequential(nn.Linear(284, 256), act(), nn.Linear(256, 256), act())
+        self.block3 = nn.Sequential(nn.Linear(263, 256), act(), nn.Linear(256, 256), act())
+        self.alpha_branch = nn.Sequential(nn.Linear(256, 1))
+        self.alpha_act = nn.Softplus()
+        self.color_branch = nn.Sequential(nn.Linear(280, 128), act(), nn.Linear(128, 128), act(),
+                                          nn.Linear(128, 128), act(), nn.Linear(128, 3))
+        self.color_act = nn.Sigmoid()
+        for m in self.modules():
+            if isinstance(m, nn.Linear):
+                nn.init.xavier_uniform_(m.weight)
+                nn.init.zeros_(m.bias)
+        self.chunksize = 20000  # the reference's sample chunk; the fused kernels need none
+        self._packed = None
+        self._packed_key = None
+
+    def calculate_weight(self, dist, mask=None):
+        """Inverse-distance weights over the last axis, masked entries 0 (epcq.py:432-435)."""
+        inv = 1 / (dist + 1e-6)
+        if mask is not None:
+            inv = inv * mask.float()
+        return inv / (torch.sum(inv, dim=-1, keepdim=True) + 1e-6)
+
+    def _linears(self):
+        return [self.block1[0], self.block1[2], self.block3[0], self.block3[2], self.alpha_branch[0],
+                self.color_branch[0], self.color_branch[2], self.color_branch[4], self.color_branch[6]]
+
+    def packed_weights(self):
+        """The bf16 operand tiles of the current parameters (re-packed when any of them changed)."""
+        params = [t for m in self._linears() for t in (m.weight, m.bias)]
+        key = tuple((t.data_ptr(), t._version, t.device) for t in params)
+        if self._packed is None or self._packed_key != key:
+            lin = self._linears()
+            self._packed = ops.aggregator_pack([m.weight for m in lin], [m.bias for m in lin])
+            self._packed_key = key
+        return self._packed
+
+    def forward(self, pc_xyz, pc_rgb, pc_dir, pc_feat, output_sp_xyz, valid_sp_mask_out, mask_out, rays_d):
+        """-> (alphas, colors): [H*W, S] and [H*W, S, 3] for mask_out [H, W, S] (inference), [R, S]
+        and [R, S, 3] for [R, S] (training layout); zeros where mask_out is not set."""
+        if mask_out.dim() not in (2, 3):
+            raise ValueError('mask_out shape error')
+        if torch.is_grad_enabled() and any(p.requires_grad for p in self.parameters()):
+            raise RuntimeError("Aggregator: the tensor-core forward has no backward; run it under torch.no_grad()")
+        valid = valid_sp_mask_out if valid_sp_mask_out.dtype in (torch.bool, torch.uint8) else valid_sp_mask_out.bool()
+        mask = mask_out if mask_out.dtype in (torch.bool, torch.uint8) else mask_out.bool()
+        f32 = [t.detach().to(torch.float32).contiguous() for t in (pc_xyz, pc_rgb, pc_dir, pc_feat, output_sp_xyz,
+                                                                    rays_d)]
+        return ops.aggregator_forward(self.packed_weights(), f32[0], f32[1], f32[2], f32[3], f32[4],
+                                      valid.contiguous(), mask.contiguous(), f32[5])
 
 
 def clamp_t(t_val, vsize=0.004):

@@ -24,7 +24,7 @@ LIB_NAME = "libhashpoint_b200.so"
 LIB_PATH = os.path.join(LIB_DIR, LIB_NAME)
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
-SOURCES = ["hp_api.cu", "hp_build.cu", "hp_sample.cu", "hp_query.cu", "hp_feature.cu"]
+SOURCES = ["hp_api.cu", "hp_build.cu", "hp_sample.cu", "hp_query.cu", "hp_feature.cu", "hp_aggregator.cu"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 
@@ -33,7 +33,8 @@ EXPORTS = ["hp_version", "hp_last_error", "hp_projection_rounding", "hp_pts2plan
            "hp_pts2plane_noalloc", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling",
            "hp_quick_sampling_batch_workspace_size", "hp_quick_sampling_batch", "hp_quick_query_for_nearby_point",
            "hp_scatter", "hp_ray_directions", "hp_mask_scan", "hp_mask_scan_workspace_size", "hp_feature_query",
-           "hp_clamp_t", "hp_render"]
+           "hp_clamp_t", "hp_render", "hp_aggregator_packed_size", "hp_aggregator_pack",
+           "hp_aggregator_workspace_size", "hp_aggregator_forward", "hp_aggregator_status"]
 
 HP_OK = 0
 
@@ -110,6 +111,11 @@ class HpPointAttrs(ctypes.Structure):
                 ("feat_dim", ctypes.c_int32), ("feat_half", ctypes.c_int32), ("n_points", ctypes.c_int64)]
 
 
+class HpAggregatorWeights(ctypes.Structure):
+    """The Aggregator's nine nn.Linear layers (weight [out, in], bias), module order."""
+    _fields_ = [("weight", ctypes.c_void_p * 9), ("bias", ctypes.c_void_p * 9)]
+
+
 class HpTuning(ctypes.Structure):
     """Launch tuning of hp_quick_sampling_batch (0 = default)."""
     _fields_ = [("heavy_window", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32)]
@@ -173,6 +179,17 @@ def lib():
         L.hp_clamp_t.restype = i32
         L.hp_render.argtypes = [vp, vp, ctypes.c_float, vp, vp, i64, i32, i32, vp, vp]
         L.hp_render.restype = i32
+        L.hp_aggregator_packed_size.argtypes = []
+        L.hp_aggregator_packed_size.restype = sz
+        L.hp_aggregator_pack.argtypes = [ctypes.POINTER(HpAggregatorWeights), vp, sz, vp]
+        L.hp_aggregator_pack.restype = i32
+        L.hp_aggregator_workspace_size.argtypes = [i64]
+        L.hp_aggregator_workspace_size.restype = sz
+        L.hp_aggregator_forward.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp, vp, i64, i32, vp, vp, i64, vp, vp, vp,
+                                            sz, vp]
+        L.hp_aggregator_forward.restype = i32
+        L.hp_aggregator_status.argtypes = [vp, i64, vp]
+        L.hp_aggregator_status.restype = i32
         L.hp_quick_query_for_nearby_point.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, i64, vp, vp]
         L.hp_quick_query_for_nearby_point.restype = i32
         L.hp_scatter.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp]

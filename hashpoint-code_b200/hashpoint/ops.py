@@ -336,3 +336,77 @@ def render(deltas, sigmas, rgbs, white_bg=False, t_val=None, vsize=0.004):
                                 int(bool(white_bg)), _ptr(color), _stream(sigmas.device))
     native.check(rc, "hp_render")
     return color
+
+
+# ---------------------------------------------------------------------------
+# Aggregator (epcq/epcq.py:406-507) on the tensor cores
+# ---------------------------------------------------------------------------
+# the nine nn.Linear layers in module order: (name, out, in)
+AGG_LAYERS = (("block1.0", 256, 284), ("block1.2", 256, 256), ("block3.0", 256, 263), ("block3.2", 256, 256),
+              ("alpha_branch.0", 1, 256), ("color_branch.0", 128, 280), ("color_branch.2", 128, 128),
+              ("color_branch.4", 128, 128), ("color_branch.6", 3, 128))
+
+
+def aggregator_pack(weights, biases):
+    """Pack the Aggregator's nine layers (fp32 weight [out, in] and bias [out] device tensors, module
+    order) into the bf16 operand tiles + fp32 parameters the forward kernels read (uint8 tensor)."""
+    if len(weights) != 9 or len(biases) != 9:
+        raise RuntimeError("aggregator_pack: nine layers expected")
+    w = native.HpAggregatorWeights()
+    keep = []
+    for i, ((name, n_out, n_in), W, b) in enumerate(zip(AGG_LAYERS, weights, biases)):
+        W = W.detach().to(torch.float32).contiguous()
+        b = b.detach().to(torch.float32).contiguous()
+        if tuple(W.shape) != (n_out, n_in) or tuple(b.shape) != (n_out,) or not W.is_cuda or not b.is_cuda:
+            raise RuntimeError("aggregator_pack: %s must be CUDA fp32 [%d, %d] with bias [%d]" %
+                               (name, n_out, n_in, n_out))
+        keep += [W, b]
+        w.weight[i] = W.data_ptr()
+        w.bias[i] = b.data_ptr()
+    dev = keep[0].device
+    L = native.lib()
+    size = L.hp_aggregator_packed_size()
+    packed = torch.empty(size, dtype=torch.uint8, device=dev)
+    rc = L.hp_aggregator_pack(ctypes.byref(w), _ptr(packed), size, _stream(dev))
+    native.check(rc, "hp_aggregator_pack")
+    packed._hp_keep = keep  # the sources stay alive until the packing kernel has run
+    return packed
+
+
+def aggregator_forward(packed, pc_xyz, pc_rgb, pc_dir, pc_feat, output_sp_xyz, valid_sp_mask_out, mask_out, rays_d,
+                       check_status=False):
+    """Aggregator.forward (epcq/epcq.py:441-507) on the GPU: (alphas, colors) -- [H*W, S] and
+    [H*W, S, 3] for a sampling mask [H, W, S], [R, S] and [R, S, 3] for [R, S] -- zeros where
+    mask_out is not set.  bf16 operands, fp32 accumulation.  check_status synchronises and raises
+    if a wait inside the kernels gave up."""
+    for t, nme in ((pc_xyz, "pc_xyz"), (pc_rgb, "pc_rgb"), (pc_dir, "pc_dir"), (pc_feat, "pc_feat"),
+                   (output_sp_xyz, "output_sp_xyz"), (rays_d, "rays_d")):
+        check_input(t, nme, torch.float32)
+    check_input(valid_sp_mask_out, "valid_sp_mask_out")
+    check_input(mask_out, "mask_out")
+    if mask_out.dim() not in (2, 3):
+        raise ValueError("mask_out shape error")
+    if valid_sp_mask_out.dim() != 2:
+        raise RuntimeError("valid_sp_mask_out must be [samples, points]")
+    M, P = valid_sp_mask_out.shape
+    if (pc_xyz.shape != (M, P, 3) or pc_rgb.shape != (M, P, 3) or pc_dir.shape != (M, P, 3) or
+            pc_feat.dim() != 3 or pc_feat.shape[:2] != (M, P) or output_sp_xyz.shape != (M, 3) or
+            rays_d.shape != (M, 3)):
+        raise RuntimeError("aggregator: inputs do not match valid_sp_mask_out [%d, %d]" % (M, P))
+    dev = pc_xyz.device
+    S = mask_out.shape[-1]
+    rows = mask_out.numel() // max(S, 1)
+    alphas = torch.empty((rows, S), dtype=torch.float32, device=dev)
+    colors = torch.empty((rows, S, 3), dtype=torch.float32, device=dev)
+    offsets, _ = mask_scan(mask_out)
+    L = native.lib()
+    ws_bytes = L.hp_aggregator_workspace_size(M)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    rc = L.hp_aggregator_forward(_ptr(packed), _ptr(pc_xyz), _ptr(pc_rgb), _ptr(pc_dir), _ptr(pc_feat),
+                                 int(pc_feat.shape[2]), _ptr(output_sp_xyz), _ptr(valid_sp_mask_out), _ptr(rays_d),
+                                 M, P, _ptr(mask_out), _ptr(offsets), mask_out.numel(), _ptr(alphas), _ptr(colors),
+                                 _ptr(ws), ws_bytes, _stream(dev))
+    native.check(rc, "hp_aggregator_forward")
+    if check_status:
+        native.check(L.hp_aggregator_status(_ptr(ws), M, _stream(dev)), "hp_aggregator_forward")
+    return alphas, colors

@@ -192,6 +192,41 @@ HP_API int32_t hp_render(const float* deltas, const float* t_val, float vsize, c
                          const float* rgbs, int64_t n_rays, int32_t S, int32_t white_bg, float* color,
                          hp_stream_t stream);
 
+/* Aggregator (epcq/epcq.py:406-507): the per-point MLP, alpha branch,
+ * inverse-distance aggregation and colour branch over FeatureQuery's outputs,
+ * on the tensor cores (bf16 operands, fp32 accumulation).
+ *
+ * The nine nn.Linear layers as row-major fp32 [out, in] device arrays and
+ * their biases, in module order: block1.0 (256x284), block1.2 (256x256),
+ * block3.0 (256x263), block3.2 (256x256), alpha_branch.0 (1x256),
+ * color_branch.0 (128x280), .2 (128x128), .4 (128x128), .6 (3x128). */
+typedef struct hp_aggregator_weights {
+  const float* weight[9];
+  const float* bias[9];
+} hp_aggregator_weights;
+
+/* Bytes of the packed weights (bf16 operand tiles + fp32 biases). */
+HP_API size_t hp_aggregator_packed_size(void);
+/* Pack the weights once (after every change); packed: 256-byte aligned. */
+HP_API int32_t hp_aggregator_pack(const hp_aggregator_weights* w, void* packed, size_t packed_bytes,
+                                  hp_stream_t stream);
+HP_API size_t hp_aggregator_workspace_size(int64_t n_samples);
+/* Aggregator.forward: n_samples valid samples (FeatureQuery's M) with P points
+ * each -- pc_xyz / pc_rgb / pc_dir f32 [M, P, 3], pc_feat f32 [M, P, 32]
+ * (16-byte aligned), sp_xyz and rays_d f32 [M, 3], valid u8 [M, P] -- then
+ * alpha_out f32 [n_positions] and color_out f32 [n_positions, 3]: sample
+ * mask_offsets[i] at every set position i of mask_out (the sampling mask,
+ * mask_offsets from hp_mask_scan of it), zeros elsewhere.  P: 1, 2, 4, ..., 32.
+ * Waits inside the kernels are bounded; hp_aggregator_status (synchronising)
+ * reports one that gave up. */
+HP_API int32_t hp_aggregator_forward(const void* packed, const float* pc_xyz, const float* pc_rgb,
+                                     const float* pc_dir, const float* pc_feat, int32_t feat_dim,
+                                     const float* sp_xyz, const uint8_t* valid, const float* rays_d,
+                                     int64_t n_samples, int32_t P, const uint8_t* mask_out,
+                                     const int32_t* mask_offsets, int64_t n_positions, float* alpha_out,
+                                     float* color_out, void* workspace, size_t workspace_bytes, hp_stream_t stream);
+HP_API int32_t hp_aggregator_status(const void* workspace, int64_t n_samples, hp_stream_t stream);
+
 /* Scratch bytes hp_quick_sampling needs for n_sorted ids and an image of this
  * size (its tile schedule and the ids' points packed as 16-byte records);
  * workspace must be 256-byte aligned. */

@@ -1,10 +1,12 @@
 """CPU oracle (test infrastructure only) for the rows downstream of sampling:
-FeatureQuery.forward's gather, clamp_t and render.
+FeatureQuery.forward's gather, clamp_t, render and the Aggregator MLP.
 
 Each function restates the reference's torch code in float32 numpy:
-  feature_query  epcq/epcq.py:333-387  (generate_rays :333-341, forward :344-387)
-  clamp_t        epcq/epcq.py:508-515
-  render         epcq/epcq.py:517-529
+  feature_query        epcq/epcq.py:333-387  (generate_rays :333-341, forward :344-387)
+  clamp_t              epcq/epcq.py:508-515
+  render               epcq/epcq.py:517-529
+  positional_encoding  epcq/epcq.py:389-404  (ori=False)
+  aggregator           epcq/epcq.py:406-507  (Aggregator.forward)
 Gathers and copies are exact.  Ray directions, opacities and colours are
 float32 expressions whose summation order (torch.sum, torch.cumprod) is not
 specified by the reference, so they agree with it to within a few ulp; the
@@ -70,3 +72,80 @@ def render(deltas, sigmas, rgbs, white_bg=False):
         trans = (trans * ((f32(1) - op[:, k]) + f32(1e-10))).astype(f32)
     bg = f32(1) if white_bg else f32(0)
     return (col + last[:, None] * bg).astype(f32)
+
+
+# the Aggregator's nn.Linear layers in module order: (name, out, in)
+AGG_LAYERS = (("block1.0", 256, 284), ("block1.2", 256, 256), ("block3.0", 256, 263), ("block3.2", 256, 256),
+              ("alpha_branch.0", 1, 256), ("color_branch.0", 128, 280), ("color_branch.2", 128, 128),
+              ("color_branch.4", 128, 128), ("color_branch.6", 3, 128))
+
+
+def positional_encoding(x, freqs):
+    """[..., C] -> [..., 2 C freqs]: for channel c and band f (index c * freqs + f), sin and cos of
+    x_c * 2^f, interleaved (epcq.py:389-404 with ori=False)."""
+    f32 = np.float32
+    x = np.asarray(x, f32)
+    bands = (f32(2) ** np.arange(freqs)).astype(f32)
+    p = (x[..., None] * bands).reshape(x.shape[:-1] + (freqs * x.shape[-1],)).astype(f32)
+    return np.stack([np.sin(p), np.cos(p)], -1).reshape(p.shape[:-1] + (2 * p.shape[-1],)).astype(f32)
+
+
+def aggregator(params, pc_xyz, pc_rgb, pc_dir, pc_feat, sp_xyz, valid, mask_out, rays_d):
+    """(alphas, colors) of Aggregator.forward (epcq.py:441-507) in float32.
+
+    params: {layer name: (weight [out, in], bias [out])}.  Inputs as FeatureQuery returns them:
+    pc_* [M, P, *], sp_xyz and rays_d [M, 3], valid [M, P]; mask_out is the sampling mask,
+    [H, W, S] (inference: alphas [H*W, S], colors [H*W, S, 3]) or [R, S] (training: [R, S],
+    [R, S, 3]).  The reference's 20000-sample chunks do not change the per-row arithmetic."""
+    f32 = np.float32
+    Wt = {k: (np.asarray(w, f32), np.asarray(b, f32)) for k, (w, b) in params.items()}
+
+    def lin(x, k):
+        return (x @ Wt[k][0].T + Wt[k][1]).astype(f32)
+
+    def leaky(x):
+        return np.where(x > 0, x, x * f32(0.01)).astype(f32)
+
+    pc_xyz, pc_rgb, pc_dir, pc_feat, sp_xyz, rays_d = (np.asarray(a, f32) for a in
+                                                        (pc_xyz, pc_rgb, pc_dir, pc_feat, sp_xyz, rays_d))
+    valid = np.asarray(valid, bool)
+    M, P = valid.shape
+    v = valid.reshape(-1)
+    dist = (pc_xyz - sp_xyz[:, None, :]).astype(f32)
+    distpow = (pc_xyz ** 2 - sp_xyz[:, None, :] ** 2).astype(f32)
+    norm = np.sqrt((dist * dist).sum(-1)).astype(f32)
+    inv = ((f32(1) / (norm + f32(1e-6))) * valid.astype(f32)).astype(f32)
+    weights = (inv / (inv.sum(-1, keepdims=True) + f32(1e-6))).astype(f32)
+
+    dist_feat = np.concatenate([dist, distpow], -1).reshape(-1, 6)[v]
+    feat_in = pc_feat.reshape(-1, pc_feat.shape[-1])[v]
+    rgb = pc_rgb.reshape(-1, 3)[v]
+    dr = pc_dir.reshape(-1, 3)[v]
+    rd = np.repeat(rays_d, P, axis=0)[v]
+    x = np.concatenate([feat_in, positional_encoding(feat_in, 3), positional_encoding(dist_feat, 5)], -1)
+    x = leaky(lin(leaky(lin(x, "block1.0")), "block1.2"))
+    x = np.concatenate([x, rgb, dr - rd, (dr * rd).sum(-1, keepdims=True)], -1).astype(f32)
+    x = leaky(lin(leaky(lin(x, "block3.0")), "block3.2"))
+    z = lin(x, "alpha_branch.0") - f32(1)
+    alphas = np.where(z > 20, z, np.log1p(np.exp(np.minimum(z, f32(20))))).astype(f32)
+    a = np.zeros((M * P, 1), f32)
+    a[v] = alphas
+    alpha_pred = (a.reshape(M, P) * weights).sum(-1, keepdims=True).astype(f32)
+    canvas = np.zeros((M * P, x.shape[1]), f32)
+    canvas[v] = x
+    canvas = (canvas.reshape(M, P, -1) * weights[..., None]).sum(-2).astype(f32)
+    c = np.concatenate([canvas, positional_encoding(rays_d, 4)], -1)
+    c = leaky(lin(c, "color_branch.0"))
+    c = leaky(lin(c, "color_branch.2"))
+    c = leaky(lin(c, "color_branch.4"))
+    c = lin(c, "color_branch.6")
+    color = ((f32(1) / (f32(1) + np.exp(-c))) * f32(1 + 2 * 0.001) - f32(0.001)).astype(f32)
+
+    m = np.asarray(mask_out, bool)
+    fa = np.zeros(m.size, f32)
+    fa[m.reshape(-1)] = alpha_pred.reshape(-1)
+    fc = np.zeros((m.size, 3), f32)
+    fc[m.reshape(-1)] = color
+    rows = m.shape[0] * m.shape[1] if m.ndim == 3 else m.shape[0]
+    S = m.shape[-1]
+    return fa.reshape(rows, S), fc.reshape(rows, S, 3)

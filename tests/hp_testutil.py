@@ -16,7 +16,8 @@ def golden_files():
 
 
 def downstream_files(kind):
-    """FeatureQuery / render fixtures (make_golden_downstream.py) of a kind ('feature' or 'render')."""
+    """FeatureQuery / render / Aggregator fixtures (make_golden_downstream.py) of a kind ('feature',
+    'render' or 'aggregator')."""
     out = []
     for f in sorted(glob.glob(os.path.join(GOLDEN_DIR, "fd_*.npz"))):
         if str(np.load(f)["kind"]) == kind:
@@ -63,3 +64,14 @@ def ray_mismatch(mask_a, idx_a, mask_b, idx_b, H, W):
 def bits(a):
     a = np.ascontiguousarray(a, np.float32)
     return a.view(np.int32)
+
+
+def aggregator_params(g):
+    """{layer: (weight, bias)} float32 of an Aggregator fixture (stored as fp16-representable fp16)."""
+    import oracle_downstream as OD
+    return {k: (g["w_" + k].astype(np.float32), g["b_" + k].astype(np.float32)) for k, _, _ in OD.AGG_LAYERS}
+
+
+def aggregator_inputs(g):
+    """(pc_xyz, pc_rgb, pc_dir, pc_feat, sp_xyz, valid) float32 / bool of an Aggregator fixture."""
+    return (g["pc_xyz"], g["pc_rgb"], g["pc_dir"], g["pc_feat"].astype(np.float32), g["sp_xyz"], g["valid"])

@@ -69,3 +69,49 @@ def test_ply_reader(tmp_path):
     p.write_bytes(hdr.encode() + rec.tobytes())
     a, c = E._read_ply_xyz_rgb(str(p))
     assert np.allclose(a, xyz) and np.allclose(c, rgb / 255.0)
+
+
+def test_aggregator_module_matches_reference_layout():
+    """Same parameter names and shapes as the reference's Aggregator (its state_dict loads), and the
+    same initialisation: built after the same seed, its weights are the reference's (the fixture holds
+    them rounded to fp16)."""
+    import numpy as np
+
+    import oracle_downstream as OD
+    from hp_testutil import downstream_files
+    torch.manual_seed(5)
+    a = E.Aggregator()
+    sd = a.state_dict()
+    assert list(sd) == [k + s for k, _, _ in OD.AGG_LAYERS for s in (".weight", ".bias")]
+    for k, n_out, n_in in OD.AGG_LAYERS:
+        assert tuple(sd[k + ".weight"].shape) == (n_out, n_in) and tuple(sd[k + ".bias"].shape) == (n_out,)
+    g = np.load(downstream_files("aggregator")[0])
+    for k, _, _ in OD.AGG_LAYERS:
+        assert np.array_equal(sd[k + ".weight"].numpy().astype(np.float16), g["w_" + k]), k
+    assert a.chunksize == 20000
+
+
+def test_aggregator_cpu_inputs_rejected():
+    a = E.Aggregator()
+    M, P = 4, 8
+    z = torch.zeros(M, P, 3)
+    with torch.no_grad(), pytest.raises(RuntimeError, match="CUDA"):
+        a(z, z, z, torch.zeros(M, P, 32), torch.zeros(M, 3), torch.ones(M, P, dtype=torch.bool),
+          torch.ones(2, 2, dtype=torch.bool), torch.zeros(M, 3))
+    with pytest.raises(RuntimeError, match="no_grad"):
+        a(z, z, z, torch.zeros(M, P, 32), torch.zeros(M, 3), torch.ones(M, P, dtype=torch.bool),
+          torch.ones(2, 2, dtype=torch.bool), torch.zeros(M, 3))
+
+
+def test_positional_encoding_matches_oracle():
+    import numpy as np
+
+    import oracle_downstream as OD
+    x = torch.randn(5, 6)
+    for ori in (False, True):
+        pe = E.positional_encoding(x, 4, ori).numpy()
+        want = OD.positional_encoding(x.numpy(), 4)
+        if ori:
+            args = (x.numpy()[..., None] * (2.0 ** np.arange(4, dtype=np.float32))).reshape(5, -1)
+            want = np.concatenate([x.numpy(), np.sin(args), np.cos(args)], -1)
+        np.testing.assert_allclose(pe, want, rtol=1e-6, atol=1e-6)

@@ -1,12 +1,18 @@
 """GPU parity of the rows downstream of sampling: the FeatureQuery gather
-(hp_mask_scan + hp_feature_query), clamp_t and render, through the C ABI and
-the drop-in epcq classes.
+(hp_mask_scan + hp_feature_query), clamp_t, render and the Aggregator, through
+the C ABI and the drop-in epcq classes.
 
 Against the reference's own outputs (tests/golden/fd_*.npz) and the oracle:
 gathered rows, sample points, validity flags and clamp_t exact; ray
 directions and colours rtol 1e-6, atol 1e-7 (float32 sums whose order the
 reference leaves to torch).  Also: full-size sampling outputs through the
 gather, float16 features, ids outside the cloud, empty masks, listed rays.
+
+The Aggregator runs its GEMMs on the tensor cores in bf16 with fp32
+accumulation, so it is compared with the reference's fp32 outputs at
+atol 5e-3 + rtol 2e-2 (a bf16 emulation of the fp32 oracle differs from the
+reference by at most 9e-4 on the fixture); positions outside the mask are
+exactly zero.
 """
 import numpy as np
 import pytest
@@ -14,10 +20,11 @@ import torch
 
 import oracle_downstream as OD
 from hashpoint import native, ops, synth
-from hp_testutil import bits, downstream_files
+from hp_testutil import aggregator_inputs, aggregator_params, bits, downstream_files
 
 pytestmark = pytest.mark.gpu
 RTOL, ATOL = 1e-6, 1e-7
+AGG_RTOL, AGG_ATOL = 2e-2, 5e-3
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -130,3 +137,128 @@ def test_epcq_feature_query_and_render_classes():
     r = np.load(downstream_files("render")[0])
     d = E.clamp_t(D(r["t_val"]), float(r["vsize"]))
     np.testing.assert_allclose(H(E.render(d, D(r["sigmas"]), D(r["rgbs"]))), r["color"], rtol=RTOL, atol=ATOL)
+
+
+def _agg_pack(params):
+    lin = [params[k] for k, _, _ in OD.AGG_LAYERS]
+    return ops.aggregator_pack([D(w) for w, b in lin], [D(b) for w, b in lin])
+
+
+def _agg_check(got, want, mask):
+    a, c = (H(t) for t in got)
+    wa, wc = want
+    assert a.shape == wa.shape and c.shape == wc.shape
+    np.testing.assert_allclose(a, wa, rtol=AGG_RTOL, atol=AGG_ATOL)
+    np.testing.assert_allclose(c, wc, rtol=AGG_RTOL, atol=AGG_ATOL)
+    unset = ~np.asarray(mask, bool).reshape(-1)
+    assert not a.reshape(-1)[unset].any() and not c.reshape(-1, 3)[unset].any()
+
+
+@pytest.mark.parametrize("path", downstream_files("aggregator"))
+def test_aggregator_vs_reference(path):
+    g = np.load(path)
+    packed = _agg_pack(aggregator_params(g))
+    ins = [D(x) for x in aggregator_inputs(g)]
+    for mask, a_key, c_key in (("mask", "alpha_train", "color_train"), ("mask3", "alpha_infer", "color_infer")):
+        got = ops.aggregator_forward(packed, *ins, D(g[mask]), D(g["rays_d"]), check_status=True)
+        _agg_check(got, (g[a_key], g[c_key]), g[mask])
+
+
+def test_epcq_aggregator_module():
+    """The drop-in module with the fixture's state loaded gives the same outputs as the ops call."""
+    from epcq import epcq as E
+    g = np.load(downstream_files("aggregator")[0])
+    params = aggregator_params(g)
+    agg = E.Aggregator().cuda()
+    agg.load_state_dict({k + s: torch.from_numpy(v) for k, (w, b) in params.items()
+                         for s, v in ((".weight", w), (".bias", b))})
+    ins = [D(x) for x in aggregator_inputs(g)]
+    with torch.no_grad():
+        a, c = agg(*ins, D(g["mask3"]), D(g["rays_d"]))
+    ref = ops.aggregator_forward(_agg_pack(params), *ins, D(g["mask3"]), D(g["rays_d"]))
+    assert torch.equal(a, ref[0]) and torch.equal(c, ref[1])
+    _agg_check((a, c), (g["alpha_infer"], g["color_infer"]), g["mask3"])
+    with torch.no_grad():  # a parameter change is re-packed
+        agg.color_branch[6].bias.add_(0.5)
+        a2, c2 = agg(*ins, D(g["mask3"]), D(g["rays_d"]))
+    assert torch.equal(a2, a) and not torch.equal(c2, c)
+
+
+def _random_agg_case(rng, M, P, rays, S, valid_p=0.7):
+    pc_xyz = rng.standard_normal((M, P, 3)).astype(np.float32) * 0.01
+    sp = rng.standard_normal((M, 3)).astype(np.float32)
+    pc_xyz += sp[:, None, :]
+    valid = rng.random((M, P)) < valid_p
+    valid[: M // 10] = False  # samples whose points are all invalid
+    pc_xyz[~valid] = 0.0
+    pc_rgb = np.where(valid[..., None], rng.random((M, P, 3)), 0).astype(np.float32)
+    pc_dir = np.where(valid[..., None], rng.standard_normal((M, P, 3)), 0).astype(np.float32)
+    pc_feat = np.where(valid[..., None], rng.standard_normal((M, P, 32)), 0).astype(np.float32)
+    rays_d = rng.standard_normal((M, 3)).astype(np.float32)
+    mask = np.zeros(rays * S, bool)
+    mask[np.sort(rng.choice(rays * S, M, replace=False))] = True
+    return (pc_xyz, pc_rgb, pc_dir, pc_feat, sp, valid), rays_d, mask.reshape(rays, S)
+
+
+@pytest.mark.parametrize("P", [1, 4, 8, 16, 32])
+def test_aggregator_points_per_sample_and_ragged_tiles(P):
+    """Other P, sample counts that leave partial tiles, samples with no valid point."""
+    rng = np.random.default_rng(40 + P)
+    params = {k: ((rng.standard_normal((o, i)) / np.sqrt(i)).astype(np.float32),
+                  (rng.standard_normal(o) * 0.1).astype(np.float32)) for k, o, i in OD.AGG_LAYERS}
+    M = 777 if P <= 8 else 301
+    ins, rays_d, mask = _random_agg_case(rng, M, P, 500, 4)
+    got = ops.aggregator_forward(_agg_pack(params), *[D(x) for x in ins], D(mask), D(rays_d), check_status=True)
+    _agg_check(got, OD.aggregator(params, *ins, mask, rays_d), mask)
+
+
+def test_aggregator_empty_and_errors():
+    rng = np.random.default_rng(3)
+    params = {k: ((rng.standard_normal((o, i)) / np.sqrt(i)).astype(np.float32), np.zeros(o, np.float32))
+              for k, o, i in OD.AGG_LAYERS}
+    packed = _agg_pack(params)
+    z3 = torch.zeros((0, 8, 3), device="cuda")
+    mask = torch.zeros((6, 5, 4), dtype=torch.bool, device="cuda")
+    a, c = ops.aggregator_forward(packed, z3, z3, z3, torch.zeros((0, 8, 32), device="cuda"),
+                                  torch.zeros((0, 3), device="cuda"), torch.zeros((0, 8), dtype=torch.bool,
+                                                                                   device="cuda"),
+                                  mask, torch.zeros((0, 3), device="cuda"), check_status=True)
+    assert a.shape == (30, 4) and c.shape == (30, 4, 3) and not a.any() and not c.any()
+    ins, rays_d, m = _random_agg_case(rng, 20, 8, 10, 4)
+    bad = [D(x) for x in ins]
+    with pytest.raises(native.HashPointError, match="feature width"):
+        ops.aggregator_forward(packed, *bad[:3], bad[3][..., :16].contiguous(), *bad[4:], D(m), D(rays_d))
+    ins3, rays_d3, m3 = _random_agg_case(rng, 20, 3, 10, 4)
+    with pytest.raises(native.HashPointError, match="points per sample"):
+        ops.aggregator_forward(packed, *[D(x) for x in ins3], D(m3), D(rays_d3))
+
+
+def test_aggregator_after_full_size_sampling():
+    """The full benchmark view: sampling -> FeatureQuery (fp16[32] features) -> Aggregator over all
+    its samples, checked against the oracle on 1024 of them."""
+    sc = synth.make_shapes(n_views=1, with_feat=True)
+    cam = sc.cameras[0]
+    rng = np.random.default_rng(8)
+    X = D(sc.xyz)
+    c2w, w2c, K = D(cam.c2w), D(cam.w2c), D(cam.K)
+    sidx, _, hsh = ops.pts2plane(X, w2c, K, cam.height, cam.width)
+    sp_xyz, pc_idx, sp_t, mask = ops.quick_sampling(X, c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width, cam.height,
+                                                    sc.options, sidx, hsh)
+    n = len(sc.xyz)
+    rgb = D(rng.random((n, 3), dtype=np.float32))
+    dr = D(rng.standard_normal((n, 3)).astype(np.float32))
+    fq = ops.feature_query(X, rgb, dr, D(sc.feat), sp_xyz, pc_idx, mask, c2w, cam.fx, cam.fy, cam.cx, cam.cy,
+                           cam.width)
+    params = {k: ((rng.standard_normal((o, i)) / np.sqrt(i)).astype(np.float32),
+                  (rng.standard_normal(o) * 0.05).astype(np.float32)) for k, o, i in OD.AGG_LAYERS}
+    alphas, colors = ops.aggregator_forward(_agg_pack(params), *fq[:6], mask, fq[6], check_status=True)
+    M = fq[0].shape[0]
+    assert M > 100000 and alphas.shape == (cam.height * cam.width, sc.options.num_sample_points_per_ray)
+    flat = H(mask).reshape(-1)
+    got_a = H(alphas).reshape(-1)[flat]
+    got_c = H(colors).reshape(-1, 3)[flat]
+    pick = np.sort(rng.choice(M, 1024, replace=False))
+    sub = [H(t)[pick] for t in fq]
+    want_a, want_c = OD.aggregator(params, *sub[:6], np.ones((1024, 1), bool), sub[6])
+    np.testing.assert_allclose(got_a[pick], want_a[:, 0], rtol=AGG_RTOL, atol=AGG_ATOL)
+    np.testing.assert_allclose(got_c[pick], want_c[:, 0], rtol=AGG_RTOL, atol=AGG_ATOL)
