@@ -382,6 +382,14 @@ def run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
     dr = torch.from_numpy(rng.standard_normal((n, 3)).astype(np.float32)).to(dev)
     S, P, F = sc.options.num_sample_points_per_ray, sc.options.num_point_cloud_per_sp, feat.shape[1]
     fq_ms, fq_bytes, r_ms, r_bytes = [], [], [], []
+    # Aggregator: seeded random weights of the reference's layer shapes
+    lay = ops.AGG_LAYERS
+    agg_w = [torch.from_numpy((rng.standard_normal((o, i)) / np.sqrt(i)).astype(np.float32)).to(dev) for _, o, i in lay]
+    agg_b = [torch.from_numpy((rng.standard_normal(o) * 0.05).astype(np.float32)).to(dev) for _, o, _ in lay]
+    packed = ops.aggregator_pack(agg_w, agg_b)
+    ag_ms, ag_alg, ag_exec = [], [], []
+    pair_flops = 2 * sum(o * i for name, o, i in lay if not name.startswith("color"))
+    color_flops = 2 * sum(o * i for name, o, i in lay if name.startswith("color"))
     with torch.cuda.stream(stream):
         for i in range(min(10, len(structs))):
             pipe.render(xyz, structs[i], stream)
@@ -410,6 +418,17 @@ def run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
             fq_ms.append(e[0].elapsed_time(e[1]))
             r_bytes.append(R * S * (4 + 4 + 12) + R * 12)
             r_ms.append(e[2].elapsed_time(e[3]))
+            for rep in range(2):  # the second is timed
+                flush.fill_(1)
+                ea = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                ea[0].record(stream)
+                ops.aggregator_forward(packed, *out[:6], mask, out[6])
+                ea[1].record(stream)
+                stream.synchronize()
+            n_valid = int(out[5].sum())
+            ag_ms.append(ea[0].elapsed_time(ea[1]))
+            ag_alg.append(n_valid * pair_flops + M * color_flops)
+            ag_exec.append(M * P * 2 * 256 * (320 + 256 + 256 + 16 + 256) + M * 2 * 128 * (320 + 128 + 128))
     fq = statistics.median(fq_ms)
     rr = statistics.median(r_ms)
     fqb = sum(fq_bytes) / len(fq_bytes)
@@ -419,7 +438,30 @@ def run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
                               "note": "includes the mask scan and the read-back of the sample count"},
             "render": {"ms_per_view": rr, "bytes_per_view": rb, "gbs": rb / (rr * 1e-3) / 1e9,
                        "frac_of_hbm": rb / (rr * 1e-3) / 1e9 / peak, "note": "clamp_t fused"},
+            "aggregator": _aggregator_figures(ag_ms, ag_alg, ag_exec),
             "views": len(fq_ms)}
+
+
+def _aggregator_figures(ms, alg, executed):
+    """Aggregator per view: algorithmic TFLOP/s (the reference's layers over its valid (sample, point)
+    pairs and samples) and the tensor-core rate actually executed (all pair rows, K padded to 64),
+    each against the measured dense bf16 peak."""
+    peak = _measured("bf16_tflops")
+    t = statistics.median(ms)
+    a = sum(alg) / len(alg)
+    x = sum(executed) / len(executed)
+    return {"ms_per_view": t, "tflops": a / (t * 1e-3) / 1e12, "executed_tflops": x / (t * 1e-3) / 1e12,
+            "peak_tflops": peak, "frac_of_peak": (a / (t * 1e-3) / 1e12) / peak if peak else None,
+            "executed_frac_of_peak": (x / (t * 1e-3) / 1e12) / peak if peak else None,
+            "note": "bf16 operands, fp32 accumulation; peak = measured burst bf16 GEMM"}
+
+
+def _measured(key):
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)[key])
+    except (OSError, KeyError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}.get(key)
 
 
 def run_other_configs(dev, flush):

@@ -2,15 +2,16 @@
 // bulk global->shared copies, TMEM allocation, tcgen05.mma (bf16 x bf16 ->
 // fp32 in TMEM) and tcgen05.ld.
 //
-// Operand layout.  Every shared-memory operand is stored in the canonical
-// K-major "no swizzle" layout of tcgen05: 8x8 core matrices (8 rows of 16
-// bytes, 128 contiguous bytes), the core matrix of row group g and K group kk
-// at byte offset g * SBO + kk * 128 (LBO = 128 bytes between K-adjacent core
-// matrices, SBO = K * 2 bytes between 8-row groups of a K-wide operand).  So
-// element (r, k) of an operand that is K wide sits at
-//   (r / 8) * (K * 16) + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2.
-// One MMA consumes 16 K (two core matrices); the next K step starts 256
-// bytes further on.
+// Operand layout.  Every shared-memory operand is stored K-major with the
+// 128-byte swizzle of tcgen05: K is cut into blocks of 64 bf16 (one 128-byte
+// row per matrix row), a block of R rows is R * 128 contiguous bytes (8-row
+// atoms of 1024 bytes, SBO = 1024), and inside a row the eight 16-byte chunks
+// are permuted by chunk ^ (row % 8).  So element (r, k) of an operand with R
+// rows sits at
+//   (k / 64) * (R * 128) + r * 128 + (((k / 8) % 8) ^ (r % 8)) * 16 + (k % 8) * 2.
+// Blocks start 1024-byte aligned.  One MMA consumes 16 K; within a block the
+// next K step starts 32 bytes further on (the swizzle is applied to the
+// address bits, so the descriptor's start address simply advances).
 //
 // Waits are bounded: every mbarrier wait gives up after kWaitNs of
 // %globaltimer and reports failure, so a kernel whose copies or MMAs never
@@ -58,6 +59,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // Wait until the phase of the given parity has completed; false after kWaitNs.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
   if (mbar_try_wait(bar, parity)) return true;
@@ -95,11 +100,31 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 // --- descriptors -------------------------------------------------------------
-// Shared-memory matrix descriptor: start address, LBO, SBO (all >> 4), version
-// 1 (bits 46-47), base offset 0, no swizzle (bits 61-63 = 0).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+// Shared-memory matrix descriptor of a K-major 128-byte-swizzled operand:
+// start address >> 4 (bits 0-13), LBO 16 bytes (unused inside one swizzle
+// row; bits 16-29), SBO 1024 bytes between 8-row atoms (bits 32-45), version
+// 1 (bits 46-47), base offset 0, layout SWIZZLE_128B = 2 (bits 61-63).
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+  const uint64_t lo = (uint64_t)((addr >> 4) & 0x3fffu) | ((uint64_t)1 << 16);
+  const uint64_t hi = (uint64_t)(1024u >> 4) | (1ull << 14) | (2ull << 29);
+  return lo | (hi << 32);
+}
+
+// Descriptor of a K-major operand in the canonical no-swizzle layout (8x8
+// core matrices of 128 contiguous bytes): lbo = bytes between K-adjacent core
+// matrices, sbo = bytes between 8-row groups; layout type 0.
+__device__ __forceinline__ uint64_t smem_desc_plain(uint32_t addr, uint32_t lbo, uint32_t sbo) {
   const uint64_t lo = (uint64_t)((addr >> 4) & 0x3fffu) | ((uint64_t)((lbo >> 4) & 0x3fffu) << 16);
   const uint64_t hi = (uint64_t)((sbo >> 4) & 0x3fffu) | (1ull << 14);
+  return lo | (hi << 32);
+}
+
+// Descriptor of a K-major 64-byte-swizzled operand: rows of 32 bf16 (64
+// bytes), 8-row atoms of 512 bytes (SBO), the 16-byte chunks of a row permuted
+// by chunk ^ ((row / 2) % 4); layout SWIZZLE_64B = 4 (bits 61-63).
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr) {
+  const uint64_t lo = (uint64_t)((addr >> 4) & 0x3fffu) | ((uint64_t)1 << 16);
+  const uint64_t hi = (uint64_t)(512u >> 4) | (1ull << 14) | (4ull << 29);
   return lo | (hi << 32);
 }
 
@@ -144,9 +169,35 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// Byte offset of element (r, k) in a canonical K-major operand K elements wide.
-__host__ __device__ __forceinline__ uint32_t operand_offset(int r, int k, int K) {
-  return (uint32_t)((r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+// Byte offset of element (n, k), k < 32, in a K-major 64-byte-swizzled block.
+__host__ __device__ __forceinline__ uint32_t sw64_offset(int n, int k) {
+  return (uint32_t)(n * 64 + ((((k >> 3) & 3) ^ ((n >> 1) & 3)) << 4) + (k & 7) * 2);
+}
+
+// Byte offset of element (r, k) of a 16-wide K-major operand in the no-swizzle
+// layout (lbo 128, sbo 256).
+__host__ __device__ __forceinline__ uint32_t plain16_offset(int r, int k) {
+  return (uint32_t)((r >> 3) * 256 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// Barrier 1 over the first n threads of the block (warps 0 .. n/32 - 1), with
+// an OR of pred over them returned to all.
+__device__ __forceinline__ int named_sync_or(int pred, int n) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.s32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.s32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"(pred), "r"(n)
+      : "memory");
+  return r;
+}
+
+// Byte offset of element (r, k) in a K-major 128-byte-swizzled operand of R rows.
+__host__ __device__ __forceinline__ uint32_t operand_offset(int r, int k, int R) {
+  return (uint32_t)((k >> 6) * (R * 128) + r * 128 + ((((k >> 3) & 7) ^ (r & 7)) << 4) + (k & 7) * 2);
 }
 
 }  // namespace tc
