@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=1000)
     ap.add_argument("--kernels-once", action="store_true",
                     help="run one view of the workload once through every kernel of the path and exit (for profilers)")
+    ap.add_argument("--agg-case", type=int, default=0, metavar="N",
+                    help="run the Aggregator twice on N seeded random samples (8 points each) and exit (for profilers)")
     return ap.parse_args()
 
 
@@ -258,13 +260,13 @@ def run_gpu(args):
     # the two system forms beside the plain per-view launch (one GPU runs them alone)
     batched = served = downstream = others = None
     if world == 1 and not args.no_systems:
+        served = run_served(args, dev)  # first: the real-time loop is the most sensitive to the process's state
+        torch.cuda.empty_cache()
         downstream = run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
         others = run_other_configs(dev, flush)
         del pipe
         torch.cuda.empty_cache()
         batched = run_batched(args, dev, xyz, sc, flush)
-        torch.cuda.empty_cache()
-        served = run_served(args, dev)
         torch.cuda.empty_cache()
 
     result = {
@@ -562,9 +564,20 @@ def run_served(args, dev):
                                       synth.MIXED_RESOLUTIONS)
 
     budget = 120 << 30
+    torch.cuda.empty_cache()
     serve.Server(store, budget).run(requests(2000.0, n))  # warm: hash-table cache and allocator
-    hot = serve.Server(store, budget).run(requests(2000.0, n))
-    light = serve.Server(store, budget).run(requests(200.0, max(n // 3, 10)))
+
+    def median_run(rate, count, runs=3):
+        # batch formation under a Poisson arrival stream depends on timing, so single runs vary by
+        # +-20%: report the run with the median rays/s and the spread
+        res = sorted((serve.Server(store, budget).run(requests(rate, count)) for _ in range(runs)),
+                     key=lambda r: r["rays_per_s"] or 0)
+        med = dict(res[len(res) // 2])
+        med["runs_rays_per_s"] = [r["rays_per_s"] for r in res]
+        return med
+
+    hot = median_run(2000.0, n)
+    light = median_run(200.0, max(n // 3, 10))
     # the same requests through serial plain launches (cached tables, one request at a time)
     reqs = requests(2000.0, n)
     mk = lambda b: torch.empty(max(b, 1), dtype=torch.uint8, device=dev)
@@ -580,13 +593,14 @@ def run_served(args, dev):
 
     ser = _event_ms(serial, 1)
     rays = sum(q.rays for q in reqs)
-    keep = ("requests", "done", "rejected", "batches", "p50_ms", "p99_ms", "mean_ms", "rays_per_s", "span_ms")
+    keep = ("requests", "done", "rejected", "batches", "p50_ms", "p99_ms", "mean_ms", "rays_per_s", "span_ms",
+            "runs_rays_per_s")
     return {"scenes": len(clouds), "points": int(sum(len(c) for c in clouds)), "budget_gb": 120,
             "lambda_2000": {k: hot[k] for k in keep}, "lambda_200": {k: light[k] for k in keep},
             "serial_plain_rays_per_s": rays / (ser * 1e-3), "serial_plain_ms": ser,
             "speedup_vs_serial_plain": (hot["rays_per_s"] or 0) / (rays / (ser * 1e-3)),
-            "note": "at 2000 requests/s the offered load exceeds the GPU's capacity, so latency is mostly "
-                    "queueing; 200 requests/s is below it"}
+            "note": "median of 3 runs each; at 2000 requests/s the offered load exceeds the GPU's capacity, "
+                    "so latency is mostly queueing; 200 requests/s is below it"}
 
 
 def run_reference(args):
@@ -615,8 +629,9 @@ def run_reference(args):
 def run_kernels_once(args):
     """One view of the workload through every kernel once, after one untimed pass: the projection and
     hash-table build, the per-view sampling launch, a 4-view batched launch, the listed-ray query,
-    ray directions, the FeatureQuery gather (fp16[32] features), clamp_t and render.  Prints no bench
-    line: this is the command the per-kernel profiles are captured on."""
+    ray directions, the FeatureQuery gather (fp16[32] features), the Aggregator (random weights),
+    clamp_t and render.  Prints no bench line: this is the command the per-kernel profiles are
+    captured on."""
     import numpy as np
     import torch
 
@@ -639,6 +654,10 @@ def run_kernels_once(args):
     sig = torch.rand((R, S), device=dev) * 50
     rgbs = torch.rand((R, S, 3), device=dev)
     r = batch.BatchRenderer([xyz], [(0, c) for c in sc.cameras], sc.options, dev)
+    lay = ops.AGG_LAYERS
+    packed = ops.aggregator_pack(
+        [torch.from_numpy((rng.standard_normal((o, i)) / np.sqrt(i)).astype(np.float32)).to(dev) for _, o, i in lay],
+        [torch.from_numpy((rng.standard_normal(o) * 0.05).astype(np.float32)).to(dev) for _, o, _ in lay])
     for _ in range(2):  # the first pass loads the library and warms up
         sidx, _, hsh = ops.pts2plane(xyz, w2c, K, cam.height, cam.width)
         sp_xyz, pc_idx, sp_t, mask = ops.quick_sampling(xyz, c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width,
@@ -647,17 +666,51 @@ def run_kernels_once(args):
         ops.quick_query(xyz, c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width, cam.height, sc.options, sidx, hsh,
                         ray_ids)
         ops.ray_directions(c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width, cam.height)
-        ops.feature_query(xyz, rgb, dr, feat, sp_xyz, pc_idx, mask, c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width)
+        fq = ops.feature_query(xyz, rgb, dr, feat, sp_xyz, pc_idx, mask, c2w, cam.fx, cam.fy, cam.cx, cam.cy,
+                               cam.width)
+        ops.aggregator_forward(packed, *fq[:6], mask, fq[6])
         d = ops.clamp_t(sp_t.view(R, S))
         ops.render(d, sig, rgbs)
         torch.cuda.synchronize(dev)
     print("kernels-once: ok", flush=True)
 
 
+def run_agg_case(n):
+    """The Aggregator alone on n seeded random samples of 8 points (features N(0, 1), weights of the
+    reference's shapes), twice, with the status check at the end.  No bench line."""
+    import numpy as np
+    import torch
+
+    from hashpoint import native, ops
+
+    native.build()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(1)
+    P = 8
+    sp = rng.standard_normal((n, 3)).astype(np.float32)
+    pc_xyz = (sp[:, None, :] + 0.01 * rng.standard_normal((n, P, 3))).astype(np.float32)
+
+    def T(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    ins = [T(pc_xyz), T(rng.random((n, P, 3), dtype=np.float32)), T(rng.standard_normal((n, P, 3)).astype(np.float32)),
+           T(rng.standard_normal((n, P, 32)).astype(np.float32)), T(sp), T(rng.random((n, P)) < 0.75)]
+    rays_d = T(rng.standard_normal((n, 3)).astype(np.float32))
+    mask = torch.ones((n, 1), dtype=torch.bool, device=dev)
+    lay = ops.AGG_LAYERS
+    packed = ops.aggregator_pack([T((rng.standard_normal((o, i)) / np.sqrt(i)).astype(np.float32)) for _, o, i in lay],
+                                 [T((rng.standard_normal(o) * 0.05).astype(np.float32)) for _, o, _ in lay])
+    for rep in range(2):
+        ops.aggregator_forward(packed, *ins, mask, rays_d, check_status=rep == 1)
+    print("agg-case: ok, %d samples" % n, flush=True)
+
+
 def main():
     args = parse()
     if args.kernels_once:
         run_kernels_once(args)
+    elif args.agg_case > 0:
+        run_agg_case(args.agg_case)
     elif args.impl == "reference":
         run_reference(args)
     else:

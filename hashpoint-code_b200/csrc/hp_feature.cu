@@ -116,10 +116,20 @@ __global__ void __launch_bounds__(kScanThreads) k_mask_offsets(const uint8_t* __
   __syncthreads();
   int run = tile_base[blockIdx.x] + incl - local;
   for (int w = 0; w < warp; w++) run += warp_sum[w];
+  int o[kScanPerThread];
 #pragma unroll
   for (int q = 0; q < kScanPerThread; q++) {
-    if (base + q < n) offsets[base + q] = run;
+    o[q] = run;
     run += v[q];
+  }
+  if (base + kScanPerThread <= n && ((uintptr_t)(offsets + base) & 15) == 0) {
+    int4* dst = reinterpret_cast<int4*>(offsets + base);  // this thread's 64 contiguous bytes
+#pragma unroll
+    for (int q = 0; q < kScanPerThread / 4; q++) dst[q] = make_int4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < kScanPerThread; q++)
+      if (base + q < n) offsets[base + q] = o[q];
   }
 }
 
@@ -219,11 +229,12 @@ __device__ __forceinline__ float clamped_gap(const float* t, int s, int S, float
   return __fadd_rn(__fmul_rn(d, __fsub_rn(1.0f, m)), __fmul_rn(m, vsize));
 }
 
+// one thread per (ray, sample): consecutive threads read and write consecutive elements
 __global__ void k_clamp_t(const float* __restrict__ t_val, int64_t rays, int S, float vsize, float* __restrict__ out) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= rays) return;
-  const float* t = t_val + r * S;
-  for (int s = 0; s < S; s++) out[r * S + s] = clamped_gap(t, s, S, vsize);
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rays * S) return;
+  const int s = (int)(i % S);
+  out[i] = clamped_gap(t_val + (i - s), s, S, vsize);
 }
 
 // render (with the deltas given, or derived from t_val by clamp_t when deltas is null)
@@ -338,10 +349,11 @@ extern "C" int32_t hp_feature_query(const hp_point_attrs* pts, const float* sp_x
 
 extern "C" int32_t hp_clamp_t(const float* t_val, int64_t n_rays, int32_t S, float vsize, float* t_dist,
                               hp_stream_t stream) {
-  if (n_rays < 0 || S < 1) return set_error(HP_ERR_INVALID_ARGUMENT, "hp_clamp_t: sizes out of range");
+  if (n_rays < 0 || S < 1 || n_rays * S >= (1ll << 39))
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_clamp_t: sizes out of range");
   if (n_rays == 0) return HP_OK;
   if (!t_val || !t_dist) return set_error(HP_ERR_INVALID_ARGUMENT, "hp_clamp_t: null pointer");
-  k_clamp_t<<<(unsigned)((n_rays + 255) / 256), 256, 0, (cudaStream_t)stream>>>(t_val, n_rays, S, vsize, t_dist);
+  k_clamp_t<<<(unsigned)((n_rays * S + 255) / 256), 256, 0, (cudaStream_t)stream>>>(t_val, n_rays, S, vsize, t_dist);
   return check_launch("k_clamp_t");
 }
 

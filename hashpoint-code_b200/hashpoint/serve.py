@@ -22,6 +22,7 @@ runs the same per-ray code, and a hash table is the same whether built for the
 request or found in the cache.
 """
 import collections
+import gc
 import ctypes
 import time
 
@@ -170,7 +171,7 @@ class Server:
     on_result(request): called with each finished request (outputs attached)
     before its outputs are released."""
 
-    def __init__(self, store, budget_bytes, streams=3, max_views=48, on_result=None, tuning=(0, 0)):
+    def __init__(self, store, budget_bytes, streams=3, max_views=16, on_result=None, tuning=(0, 0)):
         self.store = store
         self.budget = int(budget_bytes)
         self.max_views = int(max_views)
@@ -231,7 +232,18 @@ class Server:
         self.free_slots.append(b.slot)
 
     def run(self, requests, poll_s=50e-6, time_limit_s=600.0):
-        """Serve `requests` (arrival times relative to the start) in real time; returns stats."""
+        """Serve `requests` (arrival times relative to the start) in real time; returns stats.
+        Python's cyclic garbage collector is paused while the loop runs (a collection pass
+        stalls the launch loop for milliseconds) and restored afterwards."""
+        gc_was = gc.isenabled()
+        gc.disable()
+        try:
+            return self._run(requests, poll_s, time_limit_s)
+        finally:
+            if gc_was:
+                gc.enable()
+
+    def _run(self, requests, poll_s, time_limit_s):
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         waiting = collections.deque()
         inflight = []
