@@ -47,6 +47,8 @@
 // roles' waits then give up at once) and the status word.
 #include <cuda_bf16.h>
 
+#include <mutex>
+
 #include "hp_common.cuh"
 #include "hp_tc.cuh"
 
@@ -839,15 +841,26 @@ __global__ void k_agg_pack(PackArgs a, uint8_t* __restrict__ packed) {
   }
 }
 
-static int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
-                                                  cudaSuccess || n <= 0)
-      n = 148;
+// The two tensor-core kernels exceed the 48 KB default of dynamic shared
+// memory: opt them in once per device, and note the device's SM count.
+static int32_t agg_setup(unsigned pair_smem, unsigned color_smem, int* sms) {
+  static std::mutex mu;
+  static int sm_counts[128] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
+    return set_error(HP_ERR_CUDA, "hp_aggregator_forward: cudaGetDevice failed");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!sm_counts[dev]) {
+    int n = 0;
+    cudaError_t e = cudaFuncSetAttribute(k_agg_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, pair_smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_agg_color, cudaFuncAttributeMaxDynamicSharedMemorySize, color_smem);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || n <= 0)
+      return set_error(HP_ERR_CUDA, "hp_aggregator_forward: kernel set-up: %s", cudaGetErrorString(e));
+    sm_counts[dev] = n;
   }
-  return n;
+  *sms = sm_counts[dev];
+  return HP_OK;
 }
 
 }  // namespace hp
@@ -949,17 +962,11 @@ extern "C" int32_t hp_aggregator_forward(const void* packed, const float* pc_xyz
   if (cudaMemsetAsync(g.status, 0, sizeof(int), st) != cudaSuccess)
     return set_error(HP_ERR_CUDA, "%s: memset failed", who);
   if (n_samples > 0) {
-    static bool attr = false;
-    if (!attr) {
-      if (cudaFuncSetAttribute(k_agg_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, kPairSmem) != cudaSuccess ||
-          cudaFuncSetAttribute(k_agg_color, cudaFuncAttributeMaxDynamicSharedMemorySize, kColorSmem) != cudaSuccess)
-        return set_error(HP_ERR_CUDA, "%s: cudaFuncSetAttribute failed", who);
-      attr = true;
-    }
+    int sms = 0;
+    if (int32_t rc = agg_setup(kPairSmem, kColorSmem, &sms)) return rc;
     const int spt = kAggRows / P;
     const long long pair_tiles = (n_samples + spt - 1) / spt;
     const long long color_tiles = (n_samples + kAggRows - 1) / kAggRows;
-    const int sms = sm_count();
     const unsigned pg = (unsigned)(pair_tiles < sms ? pair_tiles : sms);
     const unsigned cg = (unsigned)(color_tiles < sms ? color_tiles : sms);
     k_agg_pairs<<<pg, kPairThreads, kPairSmem, st>>>(g, pair_tiles);
