@@ -73,7 +73,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
   }
 }
 
-// --- bulk copy (no tensor map, no multicast) ---------------------------------
+// --- bulk copy (no tensor map; the issuing CTA is the only destination) -------
 // bytes: a multiple of 16; both addresses 16-byte aligned.
 __device__ __forceinline__ void bulk_load(void* dst_smem, const void* src, unsigned bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
