@@ -20,8 +20,11 @@
 //                              layer-1 operand A0, and run the epilogues: read
 //                              the accumulator with tcgen05.ld, add the bias,
 //                              LeakyReLU, write the next layer's bf16 operand
-//                              A1 (block3's seven extra inputs go to a
-//                              separate 16-wide operand E);
+//                              A1 in 64-column blocks, each released to the
+//                              MMA warp by its own barrier, so the next layer
+//                              starts while later blocks are being written
+//                              (block3's seven extra inputs go to a separate
+//                              16-wide operand E);
 //                              (warp w: TMEM lane quarter w % 4, columns
 //                              64 (w / 4) .. + 63 of its row);
 //                   warp 16    issues tcgen05.mma (M 128, N 256, K 16) from
@@ -114,7 +117,7 @@ struct PairBars {
   uint64_t empty[kStages];
   uint64_t acc_full[2];  // MMA warp -> math warps: a layer completed into accumulator i
   uint64_t a0_ready;     // math warps -> MMA warp: a tile's layer-1 operand is written (256 arrivals)
-  uint64_t a1_ready;     // math warps -> MMA warp: the next layer's operand is written (256 arrivals)
+  uint64_t a1_blk[4];    // math warps -> MMA warp: 64-column block i of the next layer's operand is written
   uint64_t w3b;          // W3b landed
   uint64_t idle;         // MMA warp: everything it issued has completed
   uint32_t tmem;
@@ -339,25 +342,34 @@ __device__ __forceinline__ void build_inputs(const AggArgs& g, long long t, int 
   }
 }
 
-// Epilogue of a hidden layer: this thread's row er, columns [64 cq, 64 cq + 64) of the
-// accumulator -> LeakyReLU(x + bias) -> bf16 into the next operand (A1).
-__device__ __forceinline__ void epilogue_hidden(uint32_t acc_addr, const float* bias, uint8_t* A1, int er, int cq) {
+// Epilogue of a hidden layer, written in K order so the next layer's MMAs can
+// start on a block while later blocks are still being written: in round kb
+// every math thread converts columns 64 kb + 16 g .. + 15 (g = warp / 4) of its
+// row er -> LeakyReLU(x + bias) -> bf16 into the next operand (A1), then
+// arrives on block kb's barrier.  `last` runs before the final arrival.
+template <class Last>
+__device__ __forceinline__ void epilogue_hidden(uint32_t acc_addr, const float* bias, uint8_t* A1, int er, int g,
+                                                uint64_t* blk, Last&& last) {
 #pragma unroll 1
-  for (int cc = 0; cc < 2; cc++) {
-    const int col0 = 64 * cq + 32 * cc;
-    float v[32];
-    tc::tmem_ld32(acc_addr + (uint32_t)col0, v);
+  for (int kb = 0; kb < 4; kb++) {
+    const int col0 = 64 * kb + 16 * g;
+    float v[16];
+    tc::tmem_ld16(acc_addr + (uint32_t)col0, v);
     const float4* b4 = reinterpret_cast<const float4*>(bias + col0);
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
+    for (int q = 0; q < 4; q++) {
       const float4 b = __ldg(b4 + q);
       v[4 * q] = leaky(__fadd_rn(v[4 * q], b.x));
       v[4 * q + 1] = leaky(__fadd_rn(v[4 * q + 1], b.y));
       v[4 * q + 2] = leaky(__fadd_rn(v[4 * q + 2], b.z));
       v[4 * q + 3] = leaky(__fadd_rn(v[4 * q + 3], b.w));
     }
-#pragma unroll
-    for (int q = 0; q < 4; q++) store_unit(A1, er, col0 / 8 + q, v + 8 * q);
+    store_unit(A1, er, col0 / 8, v);
+    store_unit(A1, er, col0 / 8 + 1, v + 8);
+    if (kb == 3) last();
+    tc::tc_fence_before();
+    tc::fence_async_smem();
+    tc::mbar_arrive(&blk[kb]);
   }
 }
 
@@ -417,7 +429,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
     tc::mbar_init(&bar.acc_full[0], 1);
     tc::mbar_init(&bar.acc_full[1], 1);
     tc::mbar_init(&bar.a0_ready, kMathThreads);
-    tc::mbar_init(&bar.a1_ready, kMathThreads);
+    for (int i = 0; i < 4; i++) tc::mbar_init(&bar.a1_blk[i], kMathThreads);
     tc::mbar_init(&bar.w3b, 1);
     tc::mbar_init(&bar.idle, 1);
     bar.abort = 0;
@@ -460,14 +472,18 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
       bool ok = wait_or_abort(&bar.w3b, 0, abort);
       for (long long t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
         for (int L = 0; L < 4 && ok; L++) {
-          ok = L == 0 ? wait_or_abort(&bar.a0_ready, (a0_ph++) & 1, abort)
-                      : wait_or_abort(&bar.a1_ready, (a1_ph++) & 1, abort);
-          if (!ok) break;
-          tc::tc_fence_after();
+          if (L == 0) {
+            if (!(ok = wait_or_abort(&bar.a0_ready, (a0_ph++) & 1, abort))) break;
+            tc::tc_fence_after();
+          }
           const uint32_t acc = tmem + (uint32_t)(L & 1) * 256u;
           const uint32_t a_addr = tc::smem_addr(L == 0 ? A0 : A1);
           const int nk = pair_k(L) / kPairChunkK;
           for (int kc = 0; kc < nk; kc++, q++) {
+            if (L > 0 && (kc & 1) == 0) {  // A1's 64-column block kc / 2 is written
+              if (!(ok = wait_or_abort(&bar.a1_blk[kc >> 1], a1_ph & 1, abort))) break;
+              tc::tc_fence_after();
+            }
             const int st = (int)(q % kStages);
             if (!(ok = wait_or_abort(&bar.full[st], (unsigned)((q / kStages) & 1), abort))) break;
             tc::tc_fence_after();
@@ -480,9 +496,10 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
             }
             tc::mma_commit(&bar.empty[st]);
           }
-          if (ok && L == 2)  // block3.0's extra inputs: E (K 16) times W3b
+          if (ok && L == 2)  // block3.0's extra inputs: E (K 16, written before block 3's arrival) times W3b
             tc::mma_bf16(acc, tc::smem_desc_plain(tc::smem_addr(E), 128u, 256u),
                          tc::smem_desc_plain(tc::smem_addr(W3b), 128u, 256u), idesc, 1u);
+          if (L > 0) a1_ph++;
           tc::mma_commit(&bar.acc_full[L & 1]);
         }
       }
@@ -493,8 +510,9 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
     __syncwarp();
   } else {
     // ---- math warps: inputs, epilogues, reductions
-    const int er = 32 * (warp & 3) + lane, cq = warp >> 2;
+    const int er = 32 * (warp & 3) + lane, cq = warp >> 2;  // cq: also the column group of the epilogues
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    auto nothing = [] {};
     unsigned acc_ph[2] = {0, 0};
     int stop = 0, slot = 0;
     if (my_tiles > 0) {
@@ -506,14 +524,11 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
       // layer 1 -> A1
       if (!wait_or_abort(&bar.acc_full[0], (acc_ph[0]++) & 1, abort)) fail = true;
       tc::tc_fence_after();
-      epilogue_hidden(lane_addr, prm + kPB1, A1, er, cq);
-      tc::tc_fence_before();
-      tc::fence_async_smem();
-      tc::mbar_arrive(&bar.a1_ready);
+      epilogue_hidden(lane_addr, prm + kPB1, A1, er, cq, bar.a1_blk, nothing);
       // layer 2 -> A1, and block3's extra inputs -> E
       if (!wait_or_abort(&bar.acc_full[1], (acc_ph[1]++) & 1, abort)) fail = true;
       tc::tc_fence_after();
-      epilogue_hidden(lane_addr + 256u, prm + kPB2, A1, er, cq);
+      epilogue_hidden(lane_addr + 256u, prm + kPB2, A1, er, cq, bar.a1_blk, [&] {
       if (cq == 3) {
         const long long m = t * spt + er / P;
         const long long e = m * P + er % P;
@@ -532,16 +547,11 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
         *reinterpret_cast<uint4*>(E + tc::plain16_offset(er, 0)) = pack8(ex);
         *reinterpret_cast<uint4*>(E + tc::plain16_offset(er, 8)) = make_uint4(0, 0, 0, 0);
       }
-      tc::tc_fence_before();
-      tc::fence_async_smem();
-      tc::mbar_arrive(&bar.a1_ready);
+      });
       // layer 3 -> A1
       if (!wait_or_abort(&bar.acc_full[0], (acc_ph[0]++) & 1, abort)) fail = true;
       tc::tc_fence_after();
-      epilogue_hidden(lane_addr, prm + kPB3, A1, er, cq);
-      tc::tc_fence_before();
-      tc::fence_async_smem();
-      tc::mbar_arrive(&bar.a1_ready);
+      epilogue_hidden(lane_addr, prm + kPB3, A1, er, cq, bar.a1_blk, nothing);
       // the next tile's inputs (A0's reader, this tile's layer 1, has completed) while layer 4 runs
       if (t + gridDim.x < n_tiles) {
         build_inputs(g, t + gridDim.x, spt, A0, sc.wgt[slot ^ 1], tid);
