@@ -260,7 +260,8 @@ struct AggArgs {
 
 // Layer-1 operand units U0 .. U1-1 of row r: columns 0..31 feat, 32..223 PE(feat, 3)
 // (argument a = channel * 3 + band at columns 32 + 2a (sin), 33 + 2a (cos)), 224..283
-// PE(dist_feat, 5), 284..319 zeros.
+// PE(dist_feat, 5), 284 the constant 1 (its weight column holds block1.0's bias),
+// 285..319 zeros.
 template <int U0, int U1>
 __device__ __forceinline__ void input_units(uint8_t* A0, int r, bool in, const float* feat, const float* df) {
   float sf[3], cf[3], sd[5], cd[5];
@@ -288,6 +289,8 @@ __device__ __forceinline__ void input_units(uint8_t* A0, int r, bool in, const f
           chd = c;
         }
         x = ((col - 224) & 1) ? cd[f] : sd[f];
+      } else if (col == 284) {
+        x = 1.0f;
       }
       v[i] = in ? x : 0.0f;
     }
@@ -346,7 +349,8 @@ __device__ __forceinline__ void build_inputs(const AggArgs& g, long long t, int 
 // start on a block while later blocks are still being written: in round kb
 // every math thread converts columns 64 kb + 16 g .. + 15 (g = warp / 4) of its
 // row er -> LeakyReLU(x + bias) -> bf16 into the next operand (A1), then
-// arrives on block kb's barrier.  `last` runs before the final arrival.
+// arrives on block kb's barrier.  `last` runs before the final arrival.  bias is
+// null for the layers whose bias came in through the MMA.
 template <class Last>
 __device__ __forceinline__ void epilogue_hidden(uint32_t acc_addr, const float* bias, uint8_t* A1, int er, int g,
                                                 uint64_t* blk, Last&& last) {
@@ -355,15 +359,19 @@ __device__ __forceinline__ void epilogue_hidden(uint32_t acc_addr, const float* 
     const int col0 = 64 * kb + 16 * g;
     float v[16];
     tc::tmem_ld16(acc_addr + (uint32_t)col0, v);
-    const float4* b4 = reinterpret_cast<const float4*>(bias + col0);
+    if (bias) {
+      const float4* b4 = reinterpret_cast<const float4*>(bias + col0);
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const float4 b = __ldg(b4 + q);
-      v[4 * q] = leaky(__fadd_rn(v[4 * q], b.x));
-      v[4 * q + 1] = leaky(__fadd_rn(v[4 * q + 1], b.y));
-      v[4 * q + 2] = leaky(__fadd_rn(v[4 * q + 2], b.z));
-      v[4 * q + 3] = leaky(__fadd_rn(v[4 * q + 3], b.w));
+      for (int q = 0; q < 4; q++) {
+        const float4 b = __ldg(b4 + q);
+        v[4 * q] = __fadd_rn(v[4 * q], b.x);
+        v[4 * q + 1] = __fadd_rn(v[4 * q + 1], b.y);
+        v[4 * q + 2] = __fadd_rn(v[4 * q + 2], b.z);
+        v[4 * q + 3] = __fadd_rn(v[4 * q + 3], b.w);
+      }
     }
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = leaky(v[i]);
     store_unit(A1, er, col0 / 8, v);
     store_unit(A1, er, col0 / 8 + 1, v + 8);
     if (kb == 3) last();
@@ -524,7 +532,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
       // layer 1 -> A1
       if (!wait_or_abort(&bar.acc_full[0], (acc_ph[0]++) & 1, abort)) fail = true;
       tc::tc_fence_after();
-      epilogue_hidden(lane_addr, prm + kPB1, A1, er, cq, bar.a1_blk, nothing);
+      epilogue_hidden(lane_addr, nullptr, A1, er, cq, bar.a1_blk, nothing);  // bias: A0 column 284
       // layer 2 -> A1, and block3's extra inputs -> E
       if (!wait_or_abort(&bar.acc_full[1], (acc_ph[1]++) & 1, abort)) fail = true;
       tc::tc_fence_after();
@@ -543,6 +551,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
             dot = i == 0 ? __fmul_rn(dv, rd) : __fmaf_rn(dv, rd, dot);
           }
           ex[6] = dot;
+          ex[7] = 1.0f;  // its W3b column holds block3.0's bias
         }
         *reinterpret_cast<uint4*>(E + tc::plain16_offset(er, 0)) = pack8(ex);
         *reinterpret_cast<uint4*>(E + tc::plain16_offset(er, 8)) = make_uint4(0, 0, 0, 0);
@@ -551,7 +560,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
       // layer 3 -> A1
       if (!wait_or_abort(&bar.acc_full[0], (acc_ph[0]++) & 1, abort)) fail = true;
       tc::tc_fence_after();
-      epilogue_hidden(lane_addr, prm + kPB3, A1, er, cq, bar.a1_blk, nothing);
+      epilogue_hidden(lane_addr, nullptr, A1, er, cq, bar.a1_blk, nothing);  // bias: E column 7
       // the next tile's inputs (A0's reader, this tile's layer 1, has completed) while layer 4 runs
       if (t + gridDim.x < n_tiles) {
         build_inputs(g, t + gridDim.x, spt, A0, sc.wgt[slot ^ 1], tid);
@@ -825,11 +834,13 @@ __global__ void k_agg_pack(PackArgs a, uint8_t* __restrict__ packed) {
     while (chunk >= c0 + pair_k(L) / kPairChunkK) c0 += pair_k(L++) / kPairChunkK;
     const int col = (chunk - c0) * kPairChunkK + k;
     const int streamed = L == 2 ? 256 : pair_real_k(L);  // block3.0's columns 256.. go to W3b
-    out[e] = __float2bfloat16_rn(col < streamed ? a.w[L][(size_t)row * pair_real_k(L) + col] : 0.0f);
+    float w = col < streamed ? a.w[L][(size_t)row * pair_real_k(L) + col] : 0.0f;
+    if (L == 0 && col == 284) w = a.b[0][row];  // block1.0's bias, against the constant input column
+    out[e] = __float2bfloat16_rn(w);
   } else if (e < n_pair + n_w3b) {
     const int o = (int)(e - n_pair) * 2;  // W3b: 256 rows x 16 K, no swizzle (tc::plain16_offset)
     const int row = (o / 256) * 8 + (o % 128) / 16, col = ((o % 256) / 128) * 8 + (o % 16) / 2;
-    out[e] = __float2bfloat16_rn(col < 7 ? a.w[2][(size_t)row * 263 + 256 + col] : 0.0f);
+    out[e] = __float2bfloat16_rn(col < 7 ? a.w[2][(size_t)row * 263 + 256 + col] : col == 7 ? a.b[2][row] : 0.0f);
   } else if (e < n_pair + n_w3b + n_color) {
     int chunk, n, k;
     chunk_coords(e - n_pair - n_w3b, chunk, n, k);
