@@ -177,3 +177,26 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(native, "LIB_PATH", str(tmp_path / "nope.so"))
     with pytest.raises(native.HashPointError):
         native.lib()
+
+
+def test_aggregator_sizes_and_validation(L):
+    """The Aggregator's host-side contract: packed-weight and workspace sizes, and the argument
+    checks that run before any device work (feature width, points per sample, alignment, workspace)."""
+    packed = L.hp_aggregator_packed_size()
+    assert packed == 34 * 16384 + 8192 + 9 * 16384 + 2056 * 4  # pair chunks, W3b, colour chunks, fp32 parameters
+    assert L.hp_aggregator_workspace_size(-1) == 0
+    w0, w1 = L.hp_aggregator_workspace_size(0), L.hp_aggregator_workspace_size(1000)
+    assert 0 < w0 < w1 and w1 % 256 == 0
+    p = ctypes.c_void_p(0x100000)
+
+    def call(feat_dim=32, P=8, ws_bytes=w1, feat=p):
+        return L.hp_aggregator_forward(p, p, p, p, feat, feat_dim, p, p, p, 1000, P, p, p, 8000, p, p, p, ws_bytes, None)
+
+    assert call(feat_dim=16) == -1 and "feature width" in _err(L)
+    for P in (0, 3, 64):
+        assert call(P=P) == -1 and "points per sample" in _err(L)
+    assert call(feat=ctypes.c_void_p(0x100004)) == -1 and "aligned" in _err(L)
+    assert call(ws_bytes=w1 - 1) == -2 and "workspace" in _err(L)
+    w = native.HpAggregatorWeights()
+    assert L.hp_aggregator_pack(ctypes.byref(w), p, packed - 1, None) == -2
+    assert L.hp_aggregator_pack(ctypes.byref(w), p, packed, None) == -1 and "layer 0" in _err(L)
