@@ -173,6 +173,15 @@ def test_edge_cases():
         oi, od, oh = O.pts2plane(xyz, O.camera_from(cam), sort)
         assert np.array_equal(hsh, oh) and np.array_equal(sidx, oi) and np.array_equal(bits(sdep), bits(od))
         assert hsh[:, 1].max() == 6000
+    # three buckets above 2048 entries (the CTAs of k_sort_huge share their list)
+    cam3 = synth.look_at_camera((0, 0, 4), (0, 0, 0), 16, 12, 50.0, 50.0, 8.5, 6.5)
+    xyz3 = np.concatenate([rng.normal(size=(3000, 3)) * 0.001 + np.array([dx, 0.0, 0.0])
+                           for dx in (-0.16, 0.0, 0.16)]).astype(np.float32)
+    for sort in (False, True):
+        (sidx, sdep, hsh), _, _ = _run_case(xyz3, cam3, opt, sort)
+        oi, od, oh = O.pts2plane(xyz3, O.camera_from(cam3), sort)
+        assert np.array_equal(hsh, oh) and np.array_equal(sidx, oi) and np.array_equal(bits(sdep), bits(od))
+        assert (hsh[:, 1] > 2048).sum() == 3
     # empty cloud
     (sidx, sdep, hsh), (sp_xyz, pc_idx, sp_t, mask), _ = _run_case(np.zeros((0, 3), np.float32), cam, opt, False)
     assert sidx.size == 0 and np.all(hsh == -1) and not mask.any() and np.all(pc_idx == -1) and np.all(sp_t == 0)
