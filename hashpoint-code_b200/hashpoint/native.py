@@ -24,7 +24,8 @@ LIB_NAME = "libhashpoint_b200.so"
 LIB_PATH = os.path.join(LIB_DIR, LIB_NAME)
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
-SOURCES = ["hp_api.cu", "hp_build.cu", "hp_sample.cu", "hp_query.cu", "hp_feature.cu", "hp_aggregator.cu"]
+SOURCES = ["hp_api.cu", "hp_build.cu", "hp_sample.cu", "hp_query.cu", "hp_feature.cu", "hp_aggregator.cu",
+           "hp_tc_check.cu"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 
@@ -34,7 +35,8 @@ EXPORTS = ["hp_version", "hp_last_error", "hp_projection_rounding", "hp_pts2plan
            "hp_quick_sampling_batch_workspace_size", "hp_quick_sampling_batch", "hp_quick_query_for_nearby_point",
            "hp_scatter", "hp_ray_directions", "hp_mask_scan", "hp_mask_scan_workspace_size", "hp_feature_query",
            "hp_clamp_t", "hp_render", "hp_aggregator_packed_size", "hp_aggregator_pack",
-           "hp_aggregator_workspace_size", "hp_aggregator_forward", "hp_aggregator_status"]
+           "hp_aggregator_workspace_size", "hp_aggregator_forward", "hp_aggregator_status",
+           "hp_tc_check_image_bytes", "hp_tc_check_mma"]
 
 HP_OK = 0
 
@@ -190,6 +192,10 @@ def lib():
         L.hp_aggregator_forward.restype = i32
         L.hp_aggregator_status.argtypes = [vp, i64, vp]
         L.hp_aggregator_status.restype = i32
+        L.hp_tc_check_image_bytes.argtypes = [i32]
+        L.hp_tc_check_image_bytes.restype = sz
+        L.hp_tc_check_mma.argtypes = [vp, vp, i32, ctypes.c_uint32, i32, ctypes.c_uint32, vp, vp]
+        L.hp_tc_check_mma.restype = i32
         L.hp_quick_query_for_nearby_point.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, i64, vp, vp]
         L.hp_quick_query_for_nearby_point.restype = i32
         L.hp_scatter.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp]

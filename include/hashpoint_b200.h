@@ -301,6 +301,26 @@ HP_API int32_t hp_scatter(const int32_t* point_idx, const int32_t* point2img, co
  * the sampling kernels compute it (cam2world_ray, cuda_util.cuh:338-354). */
 HP_API int32_t hp_ray_directions(const hp_camera* cam, float* dirs, hp_stream_t stream);
 
+/* Diagnostics: a self-check of the tensor-core operand forms the Aggregator's
+ * kernels use (no counterpart in the reference).  hp_tc_check_mma runs one
+ * tcgen05.mma, d [128, 256] f32 = A [128 x 16] * B [256 x 16]^T in bf16, from
+ * device images of shared memory (A: hp_tc_check_image_bytes(0) bytes, B:
+ * hp_tc_check_image_bytes(1); 16-byte aligned).  The descriptor of each
+ * operand starts a_offset / b_offset bytes into its image, in one of three
+ * K-major forms:
+ *   HP_TC_PLAIN  no swizzle: 8-row x 16-byte core matrices, K-adjacent ones
+ *                128 bytes apart, 8-row groups 256 bytes apart;
+ *   HP_TC_SW128  128-byte swizzle: a 128-byte row per matrix row, its 16-byte
+ *                chunks permuted by chunk ^ (row % 8), 8-row atoms of 1024 bytes;
+ *   HP_TC_SW64   64-byte swizzle: a 64-byte row per matrix row, chunks permuted
+ *                by chunk ^ ((row / 2) % 4), 8-row atoms of 512 bytes.
+ * Unlike the other entry points it allocates (a 4-byte status word) and
+ * synchronises on stream. */
+enum { HP_TC_PLAIN = 0, HP_TC_SW128 = 1, HP_TC_SW64 = 2 };
+HP_API size_t hp_tc_check_image_bytes(int32_t operand);
+HP_API int32_t hp_tc_check_mma(const void* a_image, const void* b_image, int32_t a_form, uint32_t a_offset,
+                               int32_t b_form, uint32_t b_offset, float* d, hp_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

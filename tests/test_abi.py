@@ -200,3 +200,24 @@ def test_aggregator_sizes_and_validation(L):
     w = native.HpAggregatorWeights()
     assert L.hp_aggregator_pack(ctypes.byref(w), p, packed - 1, None) == -2
     assert L.hp_aggregator_pack(ctypes.byref(w), p, packed, None) == -1 and "layer 0" in _err(L)
+
+
+def test_tc_check_validation(L):
+    """The operand-form self-check's argument checks, which run before any device work."""
+    assert L.hp_tc_check_image_bytes(0) == 81920 and L.hp_tc_check_image_bytes(1) == 32768
+    p = ctypes.c_void_p(0x100000)
+    PLAIN, SW128, SW64 = 0, 1, 2
+    bad = [
+        (None, SW128, 0, SW64, 0, "null"),
+        (ctypes.c_void_p(0x100008), SW128, 0, SW64, 0, "aligned"),
+        (p, 3, 0, SW64, 0, "form"),
+        (p, SW128, 8, SW64, 0, "offset"),                     # not on a 16-byte boundary
+        (p, SW128, 65536 + 112, SW64, 0, "offset"),           # the K window leaves its 128-byte row
+        (p, SW128, 65536 + 1024, SW64, 0, "offset"),          # 128 rows past the image's end
+        (p, PLAIN, 81920 - 4080, SW64, 0, "offset"),
+        (p, SW128, 0, SW128, 128, "offset"),                  # not in an atom's first row
+        (p, SW128, 0, SW64, 48, "offset"),
+    ]
+    for a, af, ao, bf, bo, msg in bad:
+        assert L.hp_tc_check_mma(a, p, af, ao, bf, bo, p, None) == -1, (af, ao, bf, bo)
+        assert msg in _err(L)
