@@ -10,6 +10,7 @@ allocate outputs and workspaces with torch's caching allocator on the current
 device, and pass raw pointers plus torch's current CUDA stream.
 """
 import ctypes
+import fcntl
 import os
 import subprocess
 import threading
@@ -63,10 +64,25 @@ def needs_build():
 
 
 def build(force=False, verbose=False, extra_flags=()):
-    """Compile the CUDA sources for sm_100a into the in-tree shared library."""
+    """Compile the CUDA sources for sm_100a into the in-tree shared library.
+
+    Processes that build at once (the ranks of a torchrun job, test workers)
+    take turns on a lock file next to the library; each re-checks after taking
+    it, so the first one builds and the others find the library current."""
     if not force and not needs_build():
         return LIB_PATH
     os.makedirs(LIB_DIR, exist_ok=True)
+    with open(os.path.join(LIB_DIR, ".build.lock"), "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        try:
+            if not force and not needs_build():
+                return LIB_PATH
+            return _build_locked(verbose, extra_flags)
+        finally:
+            fcntl.flock(lock, fcntl.LOCK_UN)
+
+
+def _build_locked(verbose, extra_flags):
     objs = [os.path.join(LIB_DIR, os.path.basename(s) + ".o") for s in _sources()]
 
     def compile_one(pair):

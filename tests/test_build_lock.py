@@ -1,0 +1,43 @@
+"""native.build() under concurrent processes: a builder waits for the lock
+another holds, then re-checks and does not rebuild a library that became
+current meanwhile.  The compile itself is stubbed out: no nvcc runs here."""
+import fcntl
+import os
+import subprocess
+import sys
+import time
+
+from hashpoint import native
+
+CHILD = r"""
+import sys, time
+sys.path.insert(0, sys.argv[1])
+from hashpoint import native
+calls = []
+def needs_build():
+    calls.append(time.time())
+    return len(calls) == 1          # stale before the lock, current after it
+def build_locked(verbose, extra_flags):
+    raise SystemExit("rebuilt a current library")
+native.needs_build = needs_build
+native._build_locked = build_locked
+print(native.build() == native.LIB_PATH, len(calls), "%.6f" % calls[-1])
+"""
+
+
+def test_second_builder_waits_and_skips_a_current_library():
+    os.makedirs(native.LIB_DIR, exist_ok=True)
+    pkg = os.path.dirname(os.path.dirname(os.path.abspath(native.__file__)))
+    with open(os.path.join(native.LIB_DIR, ".build.lock"), "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        child = subprocess.Popen([sys.executable, "-c", CHILD, pkg], stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                 text=True)
+        time.sleep(1.0)
+        assert child.poll() is None  # blocked on the lock
+        released = time.time()
+        fcntl.flock(lock, fcntl.LOCK_UN)
+    out, err = child.communicate(timeout=60)
+    assert child.returncode == 0, err
+    ok, n_checks, t_second = out.split()
+    assert ok == "True" and n_checks == "2"
+    assert float(t_second) >= released - 0.05  # the re-check came after the lock was released
