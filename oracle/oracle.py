@@ -5,6 +5,7 @@ of the CUDA path; nothing in the product imports it.  `build()` compiles the
 C++ restatement with the Makefile next to this file.
 """
 import ctypes
+import fcntl
 import os
 import subprocess
 
@@ -36,10 +37,23 @@ class OraOptions(ctypes.Structure):
 
 
 def build(force=False):
-    src = os.path.join(HERE, "hp_oracle.cpp")
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
-        subprocess.run(["make", "-C", HERE, "-B" if force else "all"], check=True,
-                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    """make the oracle library; processes that build at once take turns on a lock file."""
+    srcs = [os.path.join(HERE, f) for f in ("hp_oracle.cpp", "hp_oracle.h")]
+
+    def stale():
+        return force or not os.path.exists(LIB_PATH) or any(os.path.getmtime(LIB_PATH) < os.path.getmtime(f)
+                                                              for f in srcs)
+
+    if stale():
+        os.makedirs(os.path.dirname(LIB_PATH), exist_ok=True)
+        with open(os.path.join(os.path.dirname(LIB_PATH), ".build.lock"), "w") as lock:
+            fcntl.flock(lock, fcntl.LOCK_EX)
+            try:
+                if stale():
+                    subprocess.run(["make", "-C", HERE, "-B" if force else "all"], check=True,
+                                   stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+            finally:
+                fcntl.flock(lock, fcntl.LOCK_UN)
     return LIB_PATH
 
 
