@@ -213,6 +213,24 @@ class NeuralPoints(nn.Module):
         self.rasterize_hashtable = _C.scatter_hashtable
         self.quick_sampling = _C.quick_sampling
 
+    def _load_ckpt(self, ckpt):
+        """Restore a 'gt_pc' cloud from a checkpoint (a dict or a path to one) (epcq.py:223-233).
+
+        The reference assigns 'sh_data' (and 'alpha_data') to attributes NeuralPoints never
+        defines, so the call fails there.  Here 'sh_data' goes to feat_data, the tensor
+        _save2torch stores under that key, so a saved cloud loads back; 'alpha_data' is kept
+        as a plain attribute.  Other pc_types raise NotImplementedError, as in the reference."""
+        if self.pc_type != "gt_pc":
+            raise NotImplementedError
+        if isinstance(ckpt, str):
+            ckpt = torch.load(ckpt)
+        self.density_data.data = ckpt["density_data"]
+        self.feat_data.data = ckpt["sh_data"]
+        self.xyz_data.data = ckpt["xyz_data"]
+        self.capacity = self.xyz_data.shape[0]
+        if "alpha_data" in ckpt:
+            self.alpha_data = ckpt["alpha_data"]
+
     def _to_cpp(self):
         spec = _C.NeuralPointsSpec()
         spec.xyz_data = self.xyz_data.data

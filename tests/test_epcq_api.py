@@ -115,3 +115,27 @@ def test_positional_encoding_matches_oracle():
             args = (x.numpy()[..., None] * (2.0 ** np.arange(4, dtype=np.float32))).reshape(5, -1)
             want = np.concatenate([x.numpy(), np.sin(args), np.cos(args)], -1)
         np.testing.assert_allclose(pe, want, rtol=1e-6, atol=1e-6)
+
+
+def test_checkpoint_round_trip(tmp_path):
+    """_save2torch then _load_ckpt restores a 'gt_pc' cloud (density, features, positions); other
+    point-cloud types raise NotImplementedError as in the reference."""
+    import numpy as np
+    p = tmp_path / "c.ply"
+    hdr = "ply\nformat binary_little_endian 1.0\nelement vertex 3\nproperty float x\nproperty float y\nproperty float z\nend_header\n"
+    p.write_bytes(hdr.encode() + np.arange(9, dtype="<f4").tobytes())
+    a = E.NeuralPoints(pc_type="gt_pc", gt_pc_path=str(p), device="cpu")
+    with torch.no_grad():
+        a.density_data.add_(torch.arange(3.0)[:, None])
+        a.feat_data.add_(1.5)
+    ck = tmp_path / "np.pth"
+    a._save2torch(str(ck))
+    b = E.NeuralPoints(pc_type="gt_pc", gt_pc_path=str(p), device="cpu")
+    b._load_ckpt(str(ck))
+    assert torch.equal(b.density_data, a.density_data) and torch.equal(b.feat_data, a.feat_data)
+    assert torch.equal(b.xyz_data, a.xyz_data) and b.capacity == 3
+    b._load_ckpt(dict(torch.load(str(ck)), alpha_data=torch.ones(3)))
+    assert torch.equal(b.alpha_data, torch.ones(3))
+    c = E.NeuralPoints(pc_type="pc", points=torch.zeros(4, 3))
+    with pytest.raises(NotImplementedError):
+        c._load_ckpt(str(ck))
