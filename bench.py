@@ -263,7 +263,7 @@ def run_gpu(args):
         served = run_served(args, dev)  # first: the real-time loop is the most sensitive to the process's state
         torch.cuda.empty_cache()
         downstream = run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
-        others = run_other_configs(dev, flush)
+        others = run_other_workloads(dev, flush)
         del pipe
         torch.cuda.empty_cache()
         batched = run_batched(args, dev, xyz, sc, flush)
@@ -287,7 +287,7 @@ def run_gpu(args):
     if downstream is not None:
         result["downstream"] = downstream
     if others is not None:
-        result["other_configs"] = others
+        result["other_workloads"] = others
     if batched is not None:
         result["batched"] = batched
     if served is not None:
@@ -466,9 +466,9 @@ def _measured(key):
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}.get(key)
 
 
-def run_other_configs(dev, flush):
-    """Configs 1 and 3 through the same plain per-view launch (CUDA events, L2 flushed):
-    the 100k-point sphere at 400x400 (k=3) and the 3M-point clusters at 1600x1200 (K=16)."""
+def run_other_workloads(dev, flush):
+    """The 100k-point sphere at 400x400 (k=3) and the 3M-point clusters at 1600x1200 (K=16) through
+    the same plain per-view launch (CUDA events, L2 flushed)."""
     import torch
 
     from hashpoint import synth
