@@ -11,6 +11,8 @@ CPU, beside its bit-exact pinning to the reference's goldens:
                 sample's point ids are listed first and lie within the radius
                 of the sample.
   ray query     at most num_point_per_ray ids, within the radius of the ray.
+  z-buffer      each pixel keeps the `bins` smallest depths of its points, in
+                ascending order, each with its own point's id; -1 padded.
 Ids repeat only where the k x k window meets the image border: the reference
 clamps the window's cells to the image, so a border cell is visited more
 than once; away from the border every id is listed once.
@@ -131,3 +133,29 @@ def test_ray_query_points_are_near_the_ray(scene):
             v = sc.xyz[ids].astype(np.float64) - o
             dist = np.linalg.norm(v - (v @ d)[:, None] * d, axis=1)
             assert np.all(dist < r * (1 + 1e-5))
+
+
+@pytest.mark.parametrize("bins", [1, 4, 8])
+def test_multibin_keeps_the_nearest_points(scene, bins):
+    sc, cam = scene
+    H, W = cam.height, cam.width
+    pid, depth = O.project(sc.xyz, cam)
+    ps, ds, ix = O.sort_by_pixel(pid, depth, H * W)
+    od, oi = O.scatter_multibin(ix, ps, ds, H, W, bins)
+    valid = oi >= 0
+    n = valid.sum(1)
+    assert np.array_equal(valid, np.arange(bins)[None, :] < n[:, None])
+    assert np.all(od[~valid] == -1)
+    inside = pid < H * W
+    per_pixel = np.bincount(pid[inside], minlength=H * W)
+    assert np.array_equal(n, np.minimum(per_pixel, bins))
+    assert np.all(np.diff(od, axis=1)[valid[:, 1:]] >= 0)
+    px, slot = np.nonzero(valid)
+    ids = oi[px, slot]
+    assert np.array_equal(pid[ids], px) and np.array_equal(depth[ids], od[px, slot])
+    # the kept depths are the pixel's smallest ones
+    order = np.lexsort((depth[inside], pid[inside]))
+    pix_sorted, dep_sorted = pid[inside][order], depth[inside][order]
+    first = np.searchsorted(pix_sorted, np.arange(H * W))
+    for p in np.nonzero(n)[0][::7]:
+        np.testing.assert_array_equal(od[p, :n[p]], dep_sorted[first[p]:first[p] + n[p]])
