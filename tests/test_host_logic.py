@@ -1,11 +1,12 @@
-"""Host-side logic of the serving loop and the batch autotuner, on the CPU:
-camera construction, byte accounting, the hash-table cache's LRU eviction and
-pinning, the synthetic request stream and the autotuner's shape classes.
+"""Host-side logic on the CPU: the serving loop's camera construction, byte
+accounting, hash-table cache (LRU eviction, pinning) and request stream; the
+autotuner's shape classes; and every entry point's rejection of host tensors.
 No device work: the cache entries and renderers here are stand-ins."""
 import collections
 import types
 
 import numpy as np
+import pytest
 import torch
 
 from hashpoint import batch, serve, synth
@@ -117,3 +118,38 @@ def test_autotuner_shape_classes():
     assert a.key(renderer(4, 800 * 800 * 4 + 1000, [1_200_000, 400_000])) == k
     assert a.key(renderer(8, 800 * 800 * 4, [1_000_000, 500_000])) != k
     assert a.key(renderer(1, 0, [0])) == (1, 0, 0, 5, 8, 8)
+
+
+def _cpu_calls():
+    from epcq import epcq as E
+    from hashpoint import ops
+    opt = synth.Options()
+    f, i, m4, K = torch.zeros(4, 3), torch.zeros(4, dtype=torch.int32), torch.eye(4), torch.eye(3)
+    h = torch.zeros(16, 2, dtype=torch.int32)
+    sp, pc, mk = torch.zeros(2, 2, 3), torch.zeros(2, 2, 8, dtype=torch.int32), torch.zeros(2, 2, dtype=torch.bool)
+    return {
+        "pts2plane": (lambda: ops.pts2plane(f, m4, K, 4, 4), "xyz"),
+        "scatter_hashtable": (lambda: ops.scatter_hashtable(i, i, torch.zeros(4), 4, 4), "point_idx"),
+        "quick_sampling": (lambda: ops.quick_sampling(f, m4, 1., 1., 2., 2., 4, 4, opt, i, h), "xyz"),
+        "quick_query": (lambda: ops.quick_query(f, m4, 1., 1., 2., 2., 4, 4, opt, i, h, i), "xyz"),
+        "scatter_multibin": (lambda: ops.scatter_multibin(i, i, torch.zeros(4), 4, 4, 5), "point_idx"),
+        "ray_directions": (lambda: ops.ray_directions(m4, 1., 1., 2., 2., 4, 4), "c2w"),
+        "mask_scan": (lambda: ops.mask_scan(torch.zeros(4, dtype=torch.bool)), "mask"),
+        "feature_query": (lambda: ops.feature_query(f, f, f, torch.zeros(4, 32), sp, pc, mk, m4, 1., 1., 2., 2., 2), "xyz"),
+        "clamp_t": (lambda: ops.clamp_t(torch.zeros(2, 8)), "t_val"),
+        "render": (lambda: ops.render(torch.zeros(2, 8), torch.zeros(2, 8), torch.zeros(2, 8, 3)), "sigmas"),
+        "aggregator_pack": (lambda: ops.aggregator_pack([torch.zeros(o, k) for _, o, k in ops.AGG_LAYERS],
+                                                        [torch.zeros(o) for _, o, _ in ops.AGG_LAYERS]), "block1.0"),
+        "_C.scatter": (lambda: E._C.scatter(i, i, torch.zeros(4), [4, 4], 5), "point_idx"),
+        "_C.scatter_hashtable": (lambda: E._C.scatter_hashtable(i, i, torch.zeros(4), (4, 4), False), "point_idx"),
+    }
+
+
+@pytest.mark.parametrize("name", sorted(_cpu_calls()))
+def test_entry_points_reject_host_tensors(name):
+    """Like the reference's TORCH_CHECKs: a tensor argument in host memory is a RuntimeError that names
+    it, raised before any device work (there is no CPU fallback)."""
+    call, arg = _cpu_calls()[name]
+    with pytest.raises(RuntimeError, match=arg) as e:
+        call()
+    assert "CUDA" in str(e.value)
