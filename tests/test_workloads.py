@@ -84,3 +84,19 @@ def test_same_seed_same_data(make):
     assert np.array_equal(a.xyz, b.xyz) and not np.array_equal(a.xyz, c.xyz)
     for ca, cb in zip(a.cameras, b.cameras):
         assert np.array_equal(ca.c2w, cb.c2w)
+
+
+def test_serving_scenes():
+    """The served scenes (here scaled down 20x): sizes log-uniform, rescaled to the total, and each
+    scene's camera poses on the radius-4 sphere looking at the origin."""
+    from hashpoint import serve
+    clouds, poses = serve.make_scenes(np.random.default_rng(0), n_scenes=16, total_points=2_000_000,
+                                      size_range=(25_000, 300_000), n_poses=16)
+    sizes = np.array([len(c) for c in clouds])
+    assert len(clouds) == 16 and abs(int(sizes.sum()) - 2_000_000) <= 16
+    assert sizes.max() / sizes.min() > 2  # uneven
+    assert len(poses) == 16 and all(len(p) == 16 for p in poses)
+    for c2w in poses[0]:
+        eye = np.asarray(c2w, np.float64)[:3, 3]
+        assert np.isclose(np.linalg.norm(eye), 4.0, rtol=1e-5)
+        np.testing.assert_allclose(np.asarray(c2w, np.float64)[:3, 2], -eye / 4.0, atol=1e-5)
