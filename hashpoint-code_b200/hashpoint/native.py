@@ -73,7 +73,10 @@ def build(force=False, verbose=False, extra_flags=()):
         return LIB_PATH
     os.makedirs(LIB_DIR, exist_ok=True)
     with open(os.path.join(LIB_DIR, ".build.lock"), "w") as lock:
-        fcntl.flock(lock, fcntl.LOCK_EX)
+        try:
+            fcntl.flock(lock, fcntl.LOCK_EX)
+        except OSError:  # a filesystem without locks: build unserialised, as before
+            return _build_locked(verbose, extra_flags)
         try:
             if not force and not needs_build():
                 return LIB_PATH

@@ -47,13 +47,18 @@ def build(force=False):
     if stale():
         os.makedirs(os.path.dirname(LIB_PATH), exist_ok=True)
         with open(os.path.join(os.path.dirname(LIB_PATH), ".build.lock"), "w") as lock:
-            fcntl.flock(lock, fcntl.LOCK_EX)
+            try:
+                fcntl.flock(lock, fcntl.LOCK_EX)
+                locked = True
+            except OSError:  # a filesystem without locks: build unserialised
+                locked = False
             try:
                 if stale():
                     subprocess.run(["make", "-C", HERE, "-B" if force else "all"], check=True,
                                    stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
             finally:
-                fcntl.flock(lock, fcntl.LOCK_UN)
+                if locked:
+                    fcntl.flock(lock, fcntl.LOCK_UN)
     return LIB_PATH
 
 
