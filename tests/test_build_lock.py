@@ -41,3 +41,15 @@ def test_second_builder_waits_and_skips_a_current_library():
     ok, n_checks, t_second = out.split()
     assert ok == "True" and n_checks == "2"
     assert float(t_second) >= released - 0.05  # the re-check came after the lock was released
+
+
+def test_builds_without_a_lock_where_the_filesystem_has_none(monkeypatch):
+    calls = []
+
+    def no_locks(*a):
+        raise OSError("locks not supported")
+
+    monkeypatch.setattr(native.fcntl, "flock", no_locks)
+    monkeypatch.setattr(native, "needs_build", lambda: True)
+    monkeypatch.setattr(native, "_build_locked", lambda verbose, extra: calls.append(1) or native.LIB_PATH)
+    assert native.build() == native.LIB_PATH and calls == [1]
