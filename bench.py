@@ -21,6 +21,13 @@ at 256^2..1600x1200) and "served" (16 resident scenes, 40M points, Poisson
 requests, continuous batching, p50/p99 latency), each against the plain
 per-view launches of the same kernels.
 
+Also on the line, outside every timed region: "reference_gpu" (the
+reference's own CUDA path, built from its sources into oracle/_ref, on the
+same GPU and views), the other workloads' rooflines, and in "cpu_baseline" the
+oracle port, the reference's own CPU point-ray searchers (KDTreeRaySearch,
+UniformGrid) on the host cores, and the FP32 path's error against the FP64
+oracle on three full-size views.
+
 --impl reference times the reference algorithm's CPU implementation (the
 oracle port, oracle/hp_oracle.cpp) on this machine's host cores on a bounded
 sample of the same workload, rank 0 only.
@@ -69,12 +76,18 @@ def config_dict(args, extra=None):
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle port on the host cores
+# CPU baseline: the oracle port on the host cores, the reference's own CPU
+# searchers, and the FP32 path's error against the FP64 oracle
 # ---------------------------------------------------------------------------
-def cpu_baseline(n_views=3, scene=None):
+def cpu_baseline(n_views=3, scene=None, searchers=True, error_views=None):
     """Oracle (C++ restatement) on `n_views` full views of the workload, all host threads.
 
-    rays/s = rays / (hash-table build time + sampling time), both on the CPU.
+    rays/s = rays / (hash-table build time + sampling time), both on the CPU; the build (one
+    thread) and the search+sample (all threads) are also reported apart.  With `searchers`, the
+    reference's own KDTreeRaySearch / UniformGrid (point_ray_search_benchmark, staged by
+    oracle/ref_cpu.py) on the 100k-point sphere workload beside it.  `error_views`: GPU outputs of
+    full-size views ({name: (xyz, cam, opt, outputs...)}) whose error against the FP64 oracle is
+    stated (oracle/error_stats.py).
     """
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -82,17 +95,36 @@ def cpu_baseline(n_views=3, scene=None):
     oracle.build()
     sc = scene or synth.make_shapes(n_views=max(n_views, 1), with_feat=False)
     cores = os.cpu_count() or 1
-    total_rays, t_total = 0, 0.0
+    total_rays, t_build, t_search = 0, 0.0, 0.0
     for cam in sc.cameras[:n_views]:
         oc = oracle.camera_from(cam)
         t0 = time.perf_counter()
         oi, od, oh = oracle.pts2plane(sc.xyz, oc, False)
+        t1 = time.perf_counter()
         oracle.quick_sampling(sc.xyz, oc, sc.options, oi, oh, nthreads=cores)
-        t_total += time.perf_counter() - t0
+        t2 = time.perf_counter()
+        t_build += t1 - t0
+        t_search += t2 - t1
         total_rays += cam.width * cam.height
-    return {"value": total_rays / t_total, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "%d full view(s) (800x800, 1M points) of the workload: hash-table build single-threaded, "
-                      "search+sample on %d threads; %.2f s wall" % (n_views, cores, t_total)}
+    t_total = t_build + t_search
+    out = {"value": total_rays / t_total, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": "%d full view(s) (800x800, 1M points) of the workload: hash-table build single-threaded "
+                     "(%.3f s), search+sample on %d threads (%.3f s); %.2f s wall" % (n_views, t_build, cores,
+                                                                                   t_search, t_total),
+           "build_s_per_view": t_build / n_views, "search_sample_rays_per_s": total_rays / t_search}
+    if searchers:
+        import ref_cpu
+        if ref_cpu.staged():
+            try:
+                out["reference_searchers"] = ref_cpu.run()
+            except Exception as e:  # noqa: BLE001 -- reported, the baseline leg goes on
+                out["reference_searchers"] = {"unavailable": str(e).splitlines()[0][:200]}
+        else:
+            out["reference_searchers"] = {"unavailable": "point_ray_search_benchmark not staged (oracle/ref_cpu.py)"}
+    if error_views:
+        import error_stats
+        out["fp64_error"] = {name: error_stats.fp64_error(*v, nthreads=cores) for name, v in error_views.items()}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -257,24 +289,32 @@ def run_gpu(args):
     # end to end through the epcq API with host buffers
     e2e = run_e2e(args, sc, dev, pipe_hw=HW)
 
-    # the two system forms beside the plain per-view launch (one GPU runs them alone)
-    batched = served = downstream = others = None
+    # the two system forms beside the plain per-view launch (one GPU runs them alone), the other
+    # workloads, and the reference's own CUDA path on the same GPU
+    batched = served = downstream = others = refgpu = error_views = None
     if world == 1 and not args.no_systems:
         served = run_served(args, dev)  # first: the real-time loop is the most sensitive to the process's state
         torch.cuda.empty_cache()
         downstream = run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
-        others = run_other_workloads(dev, flush)
+        others = run_other_workloads(dev, flush, peak)
         del pipe
+        torch.cuda.empty_cache()
+        refgpu = run_reference_gpu(dev, flush, {
+            WORKLOAD.rsplit("-", 1)[0]: ms_per_step / len(structs),
+            "sphere-100k-400x400": others["sphere_100k_400x400"]["ms_per_view"],
+            "clusters-3M-1600x1200": others["clusters_3M_1600x1200"]["ms_per_view"]})
         torch.cuda.empty_cache()
         batched = run_batched(args, dev, xyz, sc, flush)
         torch.cuda.empty_cache()
+        error_views = collect_error_views(dev)
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no public dataset)",
         "config": config_dict(args, {"l2": "flushed between steps (256 MiB write)",
-                                     "path": "plain per-view launch, preallocated buffers"}),
+                                     "path": "plain per-view launch, preallocated buffers",
+                                     "sampling_stage_config": "default (hp_tuning.stage_config 0)"}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "k_quick_sampling", "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": sum(samp_bytes) / len(samp_bytes),
@@ -292,8 +332,10 @@ def run_gpu(args):
         result["batched"] = batched
     if served is not None:
         result["served"] = served
+    if refgpu is not None:
+        result["reference_gpu"] = refgpu
     if rank == 0 and world == 1:
-        result["cpu_baseline"] = cpu_baseline()
+        result["cpu_baseline"] = cpu_baseline(searchers=not args.no_systems, error_views=error_views)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -466,9 +508,17 @@ def _measured(key):
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}.get(key)
 
 
-def run_other_workloads(dev, flush):
+def sampling_bytes(n_in, H, W, S, P):
+    """Algorithmic bytes of one k_quick_sampling launch: the in-image points' (x, y, z, id) records and
+    the hash table read once, every output element written once."""
+    HW = H * W
+    return 16 * n_in + 8 * HW + HW * S * (12 + 4 + 1 + 4 * P)
+
+
+def run_other_workloads(dev, flush, peak):
     """The 100k-point sphere at 400x400 (k=3) and the 3M-point clusters at 1600x1200 (K=16) through
-    the same plain per-view launch (CUDA events, L2 flushed)."""
+    the same plain per-view launch (CUDA events, L2 flushed before each view): build + sample per
+    view, the sampling launch alone, and its fraction of the HBM roofline."""
     import torch
 
     from hashpoint import synth
@@ -481,23 +531,107 @@ def run_other_workloads(dev, flush):
         pipe = ViewPipeline(len(sc.xyz), c0.height, c0.width, sc.options, dev)
         cams = CameraTable(sc.cameras, dev)
         structs = [cams.struct(i) for i in range(cams.n)]
+        st = torch.cuda.current_stream(dev)
+        n_in = []
         for s_ in structs:
             pipe.render(X, s_)
-        ts = []
+            n_in.append(int(pipe.hash[:, 1].clamp(min=0).sum().item()))
+        ts, ss = [], []
         for _ in range(3):
             for s_ in structs:
                 flush.fill_(1)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                pipe.render(X, s_)
-                e1.record()
-                e1.synchronize()
-                ts.append(e0.elapsed_time(e1))
-        ms = statistics.median(ts)
-        out[name] = {"rays_per_s": c0.width * c0.height / (ms * 1e-3), "ms_per_view": ms, "views": len(structs),
-                     "points": len(sc.xyz)}
+                e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                e[0].record()
+                pipe.build(X, s_, st)
+                e[1].record()
+                pipe.sample(X, s_, st)
+                e[2].record()
+                e[2].synchronize()
+                ts.append(e[0].elapsed_time(e[2]))
+                ss.append(e[1].elapsed_time(e[2]))
+        ms, sms = statistics.median(ts), statistics.median(ss)
+        S, P = sc.options.num_sample_points_per_ray, sc.options.num_point_cloud_per_sp
+        nbytes = sum(sampling_bytes(ni, c0.height, c0.width, S, P) for ni in n_in) / len(n_in)
+        achieved = nbytes / (sms * 1e-3) / 1e9
+        out[name] = {"rays_per_s": c0.width * c0.height / (ms * 1e-3), "ms_per_view": ms, "sample_ms": sms,
+                     "views": len(structs), "points": len(sc.xyz),
+                     "roofline": {"bound": "hbm", "kernel": "k_quick_sampling", "achieved": achieved, "peak": peak,
+                                  "unit": "GB/s", "frac": achieved / peak, "algorithmic_bytes_per_launch": nbytes}}
         del pipe, X
         torch.cuda.empty_cache()
+    return out
+
+
+def collect_error_views(dev):
+    """View 0 of the sphere, shapes and clusters workloads through the CUDA path, as host arrays
+    (the inputs of oracle/error_stats.fp64_error)."""
+    import torch
+
+    from hashpoint import ops, synth
+
+    out = {}
+    for name, sc in (("sphere", synth.make_sphere()), ("shapes", synth.make_shapes(n_views=1, with_feat=False)),
+                     ("clusters", synth.make_clusters(n_views=1))):
+        cam = sc.cameras[0]
+        X = torch.from_numpy(sc.xyz).to(dev)
+        c2w, w2c, K = (torch.from_numpy(a).to(dev) for a in (cam.c2w, cam.w2c, cam.K))
+        sidx, sdep, hsh = ops.pts2plane(X, w2c, K, cam.height, cam.width, False)
+        sp_xyz, pc_idx, sp_t, mask = ops.quick_sampling(X, c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width, cam.height,
+                                                        sc.options, sidx, hsh)
+        dirs = ops.ray_directions(c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width, cam.height)
+        H = lambda t: t.cpu().numpy()
+        out[name] = (sc.xyz, cam, sc.options, H(sidx), H(sdep), H(hsh), H(sp_xyz), H(sp_t), H(mask), H(pc_idx), H(dirs))
+        del X
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_reference_gpu(dev, flush, ours):
+    """The reference's own CUDA path on the same GPU and inputs: its extension (oracle/_ref, built
+    from the reference's sources) driven as epcq.py:279-325 drives it -- torch projection and
+    sort, _C.scatter_hashtable, _C.quick_sampling -- timed per view with CUDA events (L2 flushed
+    before each step of views), beside this library's plain per-view launch of the same views.
+    `ours`: {workload: ms per view} of this library."""
+    import numpy as np
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import build_ref
+    from ref_pipeline import RefPipeline
+    from hashpoint import synth
+
+    if not os.path.exists(build_ref.SO_PATH):
+        return {"unavailable": "the reference's CUDA build (oracle/_ref) is not present"}
+    rp = RefPipeline(build_ref.load(), dev)
+    out = {}
+    for name, sc, nv in (("shapes-1M-800x800", synth.make_shapes(n_views=10, with_feat=False), 10),
+                         ("sphere-100k-400x400", synth.make_sphere(), 1),
+                         ("clusters-3M-1600x1200", synth.make_clusters(n_views=4), 4)):
+        X = torch.from_numpy(sc.xyz).to(dev)
+        cams = [(torch.from_numpy(c.c2w).to(dev), torch.from_numpy(c.w2c).to(dev), torch.from_numpy(c.K).to(dev), c)
+                for c in sc.cameras[:nv]]
+        for c2w, w2c, K, c in cams:  # warm-up
+            rp.render(X, c2w, w2c, K, c, sc.options)
+        steps = []
+        for _ in range(3 if nv > 1 else 10):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for c2w, w2c, K, c in cams:
+                rp.render(X, c2w, w2c, K, c, sc.options)
+            e1.record()
+            e1.synchronize()
+            steps.append(e0.elapsed_time(e1) / nv)
+        ms = statistics.median(steps)
+        rays = sc.cameras[0].width * sc.cameras[0].height
+        out[name] = {"ms_per_view": ms, "rays_per_s": rays / (ms * 1e-3), "views": nv,
+                     "ms_per_view_here": ours.get(name), "speedup_over_reference_gpu":
+                     ms / ours[name] if ours.get(name) else None}
+        del X, cams
+        torch.cuda.empty_cache()
+    out["path"] = ("reference extension built from the reference's epcq/csrc for sm_100a, driven as epcq.py "
+                   "pts2plane + render_image_hashtable_topk (P=8); the sorted pixel ids get a sentinel element "
+                   "after the end (the reference's bucket walk reads one past them)")
     return out
 
 
@@ -610,8 +744,8 @@ def run_reference(args):
     from hashpoint import synth
     sc = synth.make_shapes(n_views=1, with_feat=False)
     for _ in range(args.warmup):
-        cpu_baseline(n_views=1, scene=sc)
-    vals = [cpu_baseline(n_views=1, scene=sc) for _ in range(args.steps)]
+        cpu_baseline(n_views=1, scene=sc, searchers=False)
+    vals = [cpu_baseline(n_views=1, scene=sc, searchers=False) for _ in range(args.steps)]
     value = sum(v["value"] for v in vals) / len(vals)
     base = dict(vals[-1])
     base["value"] = value

@@ -54,6 +54,9 @@
 
 #include "hp_common.cuh"
 #include "hp_tc.cuh"
+#ifdef HP_TESTING
+#include "../../include/hashpoint_b200_testing.h"
+#endif
 
 namespace hp {
 
@@ -141,15 +144,16 @@ struct ColorScratch {
   float opart[2][kAggRows][4];
 };
 
-// Wait for a phase; gives up (and raises the CTA's abort flag) after kWaitNs,
+// Wait for a phase; gives up (and raises the CTA's abort flag) after limit_ns,
 // or at once when another role raised it.
-__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, unsigned parity, volatile int* abort) {
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, unsigned parity, volatile int* abort,
+                                              unsigned long long limit_ns) {
   if (tc::mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = tc::global_ns();
   for (;;) {
     if (tc::mbar_try_wait(bar, parity)) return true;
     if (*abort) return false;
-    if (tc::global_ns() - t0 > tc::kWaitNs) {
+    if (tc::global_ns() - t0 > limit_ns) {
       *abort = 1;
       return false;
     }
@@ -256,6 +260,8 @@ struct AggArgs {
   float* alpha;       // [M]
   float* color;       // [M, 3]
   int* status;
+  unsigned long long wait_ns;  // limit of each wait of the pair kernel's roles (tc::kWaitNs)
+  int withhold_w3b;            // a test of those waits: W3b is never loaded, so its wait gives up
 };
 
 // Layer-1 operand units U0 .. U1-1 of row r: columns 0..31 feat, 32..223 PE(feat, 3)
@@ -454,13 +460,16 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
   if (warp == kLoadWarp) {
     // ---- weight loads: W3b once, then the pair chunk stream, 34 chunks per tile
     if (lane == 0) {
-      tc::mbar_arrive_expect_tx(&bar.w3b, kW3bBytes);
-      tc::bulk_load(W3b, g.packed + kW3bOff, kW3bBytes, &bar.w3b);
+      if (!g.withhold_w3b) {
+        tc::mbar_arrive_expect_tx(&bar.w3b, kW3bBytes);
+        tc::bulk_load(W3b, g.packed + kW3bOff, kW3bBytes, &bar.w3b);
+      }
       const long long total = my_tiles * kPairChunks;
       long long q = 0;
       for (; q < total; q++) {
         const int st = (int)(q % kStages);
-        if (q >= kStages && !wait_or_abort(&bar.empty[st], (unsigned)(((q / kStages) - 1) & 1), abort)) break;
+        if (q >= kStages && !wait_or_abort(&bar.empty[st], (unsigned)(((q / kStages) - 1) & 1), abort, g.wait_ns))
+          break;
         tc::mbar_arrive_expect_tx(&bar.full[st], kChunkBytes);
         tc::bulk_load(stages + (size_t)st * kChunkBytes, g.packed + (size_t)(q % kPairChunks) * kChunkBytes,
                       kChunkBytes, &bar.full[st]);
@@ -468,7 +477,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
       // the last copy into each stage has landed before the CTA ends
       for (long long d = q - 1; d >= 0 && d >= q - kStages; d--)
         if (!tc::mbar_wait(&bar.full[d % kStages], (unsigned)((d / kStages) & 1))) fail = true;
-      if (!tc::mbar_wait(&bar.w3b, 0)) fail = true;
+      if (!g.withhold_w3b && !tc::mbar_wait(&bar.w3b, 0)) fail = true;
     }
     __syncwarp();  // the warp's other lanes wait for lane 0 here, not at the block barrier
   } else if (warp == kMmaWarp) {
@@ -477,11 +486,11 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
       const uint32_t idesc = tc::idesc_bf16(kAggRows, kPairN);
       unsigned a0_ph = 0, a1_ph = 0;
       long long q = 0;
-      bool ok = wait_or_abort(&bar.w3b, 0, abort);
+      bool ok = wait_or_abort(&bar.w3b, 0, abort, g.wait_ns);
       for (long long t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
         for (int L = 0; L < 4 && ok; L++) {
           if (L == 0) {
-            if (!(ok = wait_or_abort(&bar.a0_ready, (a0_ph++) & 1, abort))) break;
+            if (!(ok = wait_or_abort(&bar.a0_ready, (a0_ph++) & 1, abort, g.wait_ns))) break;
             tc::tc_fence_after();
           }
           const uint32_t acc = tmem + (uint32_t)(L & 1) * 256u;
@@ -489,11 +498,11 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
           const int nk = pair_k(L) / kPairChunkK;
           for (int kc = 0; kc < nk; kc++, q++) {
             if (L > 0 && (kc & 1) == 0) {  // A1's 64-column block kc / 2 is written
-              if (!(ok = wait_or_abort(&bar.a1_blk[kc >> 1], a1_ph & 1, abort))) break;
+              if (!(ok = wait_or_abort(&bar.a1_blk[kc >> 1], a1_ph & 1, abort, g.wait_ns))) break;
               tc::tc_fence_after();
             }
             const int st = (int)(q % kStages);
-            if (!(ok = wait_or_abort(&bar.full[st], (unsigned)((q / kStages) & 1), abort))) break;
+            if (!(ok = wait_or_abort(&bar.full[st], (unsigned)((q / kStages) & 1), abort, g.wait_ns))) break;
             tc::tc_fence_after();
             const uint32_t b_addr = tc::smem_addr(stages + (size_t)st * kChunkBytes);
 #pragma unroll
@@ -530,11 +539,11 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
     }
     for (long long t = blockIdx.x; t < n_tiles && !stop; t += gridDim.x, slot ^= 1) {
       // layer 1 -> A1
-      if (!wait_or_abort(&bar.acc_full[0], (acc_ph[0]++) & 1, abort)) fail = true;
+      if (!wait_or_abort(&bar.acc_full[0], (acc_ph[0]++) & 1, abort, g.wait_ns)) fail = true;
       tc::tc_fence_after();
       epilogue_hidden(lane_addr, nullptr, A1, er, cq, bar.a1_blk, nothing);  // bias: A0 column 284
       // layer 2 -> A1, and block3's extra inputs -> E
-      if (!wait_or_abort(&bar.acc_full[1], (acc_ph[1]++) & 1, abort)) fail = true;
+      if (!wait_or_abort(&bar.acc_full[1], (acc_ph[1]++) & 1, abort, g.wait_ns)) fail = true;
       tc::tc_fence_after();
       epilogue_hidden(lane_addr + 256u, prm + kPB2, A1, er, cq, bar.a1_blk, [&] {
       if (cq == 3) {
@@ -558,7 +567,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
       }
       });
       // layer 3 -> A1
-      if (!wait_or_abort(&bar.acc_full[0], (acc_ph[0]++) & 1, abort)) fail = true;
+      if (!wait_or_abort(&bar.acc_full[0], (acc_ph[0]++) & 1, abort, g.wait_ns)) fail = true;
       tc::tc_fence_after();
       epilogue_hidden(lane_addr, nullptr, A1, er, cq, bar.a1_blk, nothing);  // bias: E column 7
       // the next tile's inputs (A0's reader, this tile's layer 1, has completed) while layer 4 runs
@@ -571,7 +580,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) k_agg_pairs(AggArgs g, long l
       // rows: the warp's 32 rows x 32 columns go through a transpose buffer (in A1, whose
       // last reader, layer 4, has completed), lane l sums column l of each sample in place,
       // and the sums are written to the colour-input rows 8 columns at a time.
-      if (!wait_or_abort(&bar.acc_full[1], (acc_ph[1]++) & 1, abort)) fail = true;
+      if (!wait_or_abort(&bar.acc_full[1], (acc_ph[1]++) & 1, abort, g.wait_ns)) fail = true;
       tc::tc_fence_after();
       {
         const float w = sc.wgt[slot][er];
@@ -941,13 +950,12 @@ extern "C" size_t hp_aggregator_workspace_size(int64_t n_samples) {
   return agg_layout(n_samples).total;
 }
 
-extern "C" int32_t hp_aggregator_forward(const void* packed, const float* pc_xyz, const float* pc_rgb,
-                                         const float* pc_dir, const float* pc_feat, int32_t feat_dim,
-                                         const float* sp_xyz, const uint8_t* valid, const float* rays_d,
-                                         int64_t n_samples, int32_t P, const uint8_t* mask_out,
-                                         const int32_t* mask_offsets, int64_t n_positions, float* alpha_out,
-                                         float* color_out, void* workspace, size_t workspace_bytes,
-                                         hp_stream_t stream) {
+static int32_t agg_forward(const void* packed, const float* pc_xyz, const float* pc_rgb, const float* pc_dir,
+                           const float* pc_feat, int32_t feat_dim, const float* sp_xyz, const uint8_t* valid,
+                           const float* rays_d, int64_t n_samples, int32_t P, const uint8_t* mask_out,
+                           const int32_t* mask_offsets, int64_t n_positions, float* alpha_out, float* color_out,
+                           void* workspace, size_t workspace_bytes, hp_stream_t stream, unsigned long long wait_ns,
+                           int withhold_w3b) {
   static const char* who = "hp_aggregator_forward";
   if (feat_dim != kFeatDim)
     return set_error(HP_ERR_INVALID_ARGUMENT, "%s: feature width %d (the layers take %d)", who, feat_dim, kFeatDim);
@@ -980,6 +988,8 @@ extern "C" int32_t hp_aggregator_forward(const void* packed, const float* pc_xyz
   g.alpha = (float*)(ws + L.alpha);
   g.color = (float*)(ws + L.color);
   g.status = (int*)(ws + L.status);
+  g.wait_ns = wait_ns;
+  g.withhold_w3b = withhold_w3b;
   if (cudaMemsetAsync(g.status, 0, sizeof(int), st) != cudaSuccess)
     return set_error(HP_ERR_CUDA, "%s: memset failed", who);
   if (n_samples > 0) {
@@ -1003,6 +1013,38 @@ extern "C" int32_t hp_aggregator_forward(const void* packed, const float* pc_xyz
   }
   return HP_OK;
 }
+
+extern "C" int32_t hp_aggregator_forward(const void* packed, const float* pc_xyz, const float* pc_rgb,
+                                         const float* pc_dir, const float* pc_feat, int32_t feat_dim,
+                                         const float* sp_xyz, const uint8_t* valid, const float* rays_d,
+                                         int64_t n_samples, int32_t P, const uint8_t* mask_out,
+                                         const int32_t* mask_offsets, int64_t n_positions, float* alpha_out,
+                                         float* color_out, void* workspace, size_t workspace_bytes,
+                                         hp_stream_t stream) {
+  return agg_forward(packed, pc_xyz, pc_rgb, pc_dir, pc_feat, feat_dim, sp_xyz, valid, rays_d, n_samples, P, mask_out,
+                     mask_offsets, n_positions, alpha_out, color_out, workspace, workspace_bytes, stream, tc::kWaitNs,
+                     0);
+}
+
+#ifdef HP_TESTING
+// Test library only (include/hashpoint_b200_testing.h): the forward with the
+// pair kernel's W3b block never loaded, so the tensor-core warp's bounded wait
+// for it gives up after wait_limit_us, every other role's wait ends at once,
+// the kernels return and hp_aggregator_status reports the failure.
+extern "C" int32_t hp_aggregator_forward_withheld(const void* packed, const float* pc_xyz, const float* pc_rgb,
+                                                  const float* pc_dir, const float* pc_feat, int32_t feat_dim,
+                                                  const float* sp_xyz, const uint8_t* valid, const float* rays_d,
+                                                  int64_t n_samples, int32_t P, const uint8_t* mask_out,
+                                                  const int32_t* mask_offsets, int64_t n_positions, float* alpha_out,
+                                                  float* color_out, void* workspace, size_t workspace_bytes,
+                                                  int32_t wait_limit_us, hp_stream_t stream) {
+  if (wait_limit_us <= 0)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_aggregator_forward_withheld: wait_limit_us must be > 0");
+  return agg_forward(packed, pc_xyz, pc_rgb, pc_dir, pc_feat, feat_dim, sp_xyz, valid, rays_d, n_samples, P, mask_out,
+                     mask_offsets, n_positions, alpha_out, color_out, workspace, workspace_bytes, stream,
+                     1000ull * (unsigned long long)wait_limit_us, 1);
+}
+#endif
 
 extern "C" int32_t hp_aggregator_status(const void* workspace, int64_t n_samples, hp_stream_t stream) {
   if (!workspace || n_samples < 0) return set_error(HP_ERR_INVALID_ARGUMENT, "hp_aggregator_status: bad arguments");

@@ -503,8 +503,11 @@ constexpr size_t kNoAllocScratchBytes =
     align256(sizeof(int2) * kNoAllocMaxPoints) + 4 * align256(sizeof(float) * kNoAllocMaxPoints) + 256;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of g_noalloc_scratch per device, looked up once per device
-// (with that device current) on its first hp_pts2plane_noalloc call.
+// Device address of g_noalloc_scratch per device.  It is looked up again on
+// every call made outside stream capture (the lookup is cheap, and a
+// cudaDeviceReset since the last call would have reloaded the module at a new
+// address); a call made while its stream is being captured uses the address
+// its device's last uncaptured call found.
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_addr[128] = {nullptr};
 }  // namespace hp
@@ -520,12 +523,18 @@ extern "C" int32_t hp_pts2plane_noalloc(const float* xyz, int64_t n_points, cons
                      "(at most %lld points and %lld pixels); use hp_pts2plane with a workspace",
                      (long long)n_points, (long long)hw, (long long)kNoAllocMaxPoints, (long long)kNoAllocMaxPixels);
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
-    return set_error(HP_ERR_CUDA, "hp_pts2plane_noalloc: cudaGetDevice failed (device %d)", dev);
+  if (cudaGetDevice(&dev) != cudaSuccess)
+    return set_error(HP_ERR_CUDA, "hp_pts2plane_noalloc: cudaGetDevice failed");
+  if (dev < 0 || dev >= 128)
+    return set_error(HP_ERR_UNSUPPORTED, "hp_pts2plane_noalloc: device ordinal %d is beyond the 128 devices it tracks",
+                     dev);
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  const bool capturing =
+      cudaStreamIsCapturing((cudaStream_t)stream, &capture) != cudaSuccess || capture != cudaStreamCaptureStatusNone;
   void* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    if (!capturing) {
       const cudaError_t e = cudaGetSymbolAddress(&g_noalloc_addr[dev], g_noalloc_scratch);
       if (e != cudaSuccess) {
         g_noalloc_addr[dev] = nullptr;
@@ -534,6 +543,11 @@ extern "C" int32_t hp_pts2plane_noalloc(const float* xyz, int64_t n_points, cons
     }
     scratch = g_noalloc_addr[dev];
   }
+  if (!scratch)
+    return set_error(HP_ERR_CUDA,
+                     "hp_pts2plane_noalloc: called under stream capture before any uncaptured call on device %d "
+                     "(make one call outside capture first)",
+                     dev);
   return hp_pts2plane(xyz, n_points, cam, sort, sorted_point_idx, sorted_depth, hash_table, scratch,
                       kNoAllocScratchBytes, stream);
 }

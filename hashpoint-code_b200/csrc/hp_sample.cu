@@ -37,7 +37,7 @@
 // when it is clear of the threshold and calls norm3df only near it (see
 // RadiusTest); the mean distance of a bin is computed only for bins the walk
 // can reach.  Tiles
-// whose halo holds more than kStageCap points read candidates straight from
+// whose halo holds more points than the stage read candidates straight from
 // global memory through the same code.
 //
 // Bin sums are accumulated in window-cell then bucket order; the reference
@@ -56,9 +56,6 @@ constexpr int kTileH = 8;    // rows per block
 constexpr int kThreads = kTileW * kTileH;
 constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
 constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
-constexpr int kStageCap = 2560;  // staged points per tile (40 KB)
-constexpr int kBlocksPerSM = 4;  // resident sampling blocks per SM (64 registers, 57 KB shared memory each)
-constexpr int kSplitWork = kStageCap;  // tiles whose halo holds more points are split into row bands
 constexpr int kItemsPerTile = kTileH * 4;  // rows, each in up to four column quarters
 #ifndef HP_BIN_LIST
 #define HP_BIN_LIST 6
@@ -88,8 +85,26 @@ struct SampleArgs {
   int heavy;  // rays with more window candidates than this are served by a whole warp
 };
 
+// Stage configurations: kCap staged points per tile, kBlocks resident blocks
+// per SM.  Shared memory per SM bounds the two together (and registers per
+// thread follow from the blocks: 64 at 4 blocks, 80 at 3, 128 at 2).  A larger
+// stage splits fewer dense tiles into row bands (less re-staging of shared
+// halo rows) but keeps fewer warps resident; which wins depends on how the
+// cloud's points spread over the image, so the launch picks one
+// (hp_tuning.stage_config) and hashpoint.batch.Autotuner searches them.
+template <int kCap_, int kBlocks_>
+struct StageCfg {
+  static constexpr int kCap = kCap_;
+  static constexpr int kBlocks = kBlocks_;
+};
+using Cfg2560x4 = StageCfg<2560, 4>;  // 40 KB stage, 4 blocks per SM (the default)
+using Cfg3712x3 = StageCfg<3712, 3>;  // 58 KB stage, 3 blocks per SM
+using Cfg5888x2 = StageCfg<5888, 2>;  // 92 KB stage, 2 blocks per SM
+constexpr int kStageConfigs = 3;      // hp_tuning.stage_config 1..3 (0 = the default, 1)
+
+template <int kCap>
 struct Stage {
-  float4 cand[kStageCap];  // x, y, z, id (as int bits; -1 = invalid id)
+  float4 cand[kCap];        // x, y, z, id (as int bits; -1 = invalid id)
   int cls[kClasses];        // rays per window-size class
   int cls_base[kClasses];   // first rank of each class
   int order[kThreads];      // pixel of each rank, heaviest class first
@@ -99,8 +114,13 @@ struct Stage {
   int next_unit;            // next work unit of the tile (see process_tile)
   unsigned kept[kMaskWords][kThreads];  // per thread: window positions pass A accepted
 };
-// kBlocksPerSM CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
-static_assert(kBlocksPerSM * (sizeof(Stage) + 16 + 1024) <= 228 * 1024, "stage too large for the blocks per SM");
+// kBlocks CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
+template <class Cfg>
+constexpr bool fits_sm() {
+  return Cfg::kBlocks * (sizeof(Stage<Cfg::kCap>) + 16 + 1024) <= 228 * 1024;
+}
+static_assert(fits_sm<Cfg2560x4>() && fits_sm<Cfg3712x3>() && fits_sm<Cfg5888x2>(),
+              "a stage configuration exceeds the shared memory of its blocks per SM");
 
 // Clipped bucket range of a hash entry: [x, x + count) within [0, n_sorted).
 __device__ __forceinline__ int2 bucket_range(int2 h, int n_sorted) {
@@ -109,9 +129,10 @@ __device__ __forceinline__ int2 bucket_range(int2 h, int n_sorted) {
 }
 
 // Candidates from the tile's shared-memory stage.
+template <int kCap>
 struct SrcStaged {
   static constexpr bool kStaged = true;
-  const Stage* st;
+  const Stage<kCap>* st;
   int rv0, ru0, nu;
   __device__ __forceinline__ int cell(int vv, int uu) const { return (vv - rv0) * nu + (uu - ru0); }
   __device__ __forceinline__ int2 range(const SampleArgs&, int vv, int uu) const {
@@ -204,9 +225,8 @@ __device__ __forceinline__ void walk_window(const SampleArgs& a, const Src& src,
 // Staged tiles, unclamped window columns: the same visit as walk_window's
 // fast path, also passing each candidate's position f in the window's
 // candidate sequence (window rows concatenated, entries in stage order).
-template <class Body>
-__device__ __forceinline__ void walk_rows(const SampleArgs& a, const SrcStaged& src, int v, int u, int cap,
-                                          Body&& body) {
+template <class Src, class Body>
+__device__ __forceinline__ void walk_rows(const SampleArgs& a, const Src& src, int v, int u, int cap, Body&& body) {
   const int H = a.cam.height, k = a.opt.k;
   const int lo = ((k + 1) >> 1) - 1;
   const int* off = src.st->off;
@@ -235,9 +255,9 @@ __device__ __forceinline__ void walk_rows(const SampleArgs& a, const SrcStaged& 
 // Visit the candidates whose window positions are set in a kept mask (nw
 // words, stride kThreads), in order; the position is mapped back to the stage
 // row by row.
-template <class Body>
-__device__ __forceinline__ void walk_kept(const SampleArgs& a, const SrcStaged& src, int v, int u,
-                                          const unsigned* mask, int nw, Body&& body) {
+template <class Src, class Body>
+__device__ __forceinline__ void walk_kept(const SampleArgs& a, const Src& src, int v, int u, const unsigned* mask,
+                                          int nw, Body&& body) {
   const int H = a.cam.height, k = a.opt.k;
   const int lo = ((k + 1) >> 1) - 1;
   const int* off = src.st->off;
@@ -1005,30 +1025,13 @@ struct Sched {
 
 __device__ __forceinline__ int cost_class(int w) { return 31 - __clz(w | 1); }
 
-// Points in the window halo of rows [vb, vb + rows) and tile columns [c0, c1) (one warp).
-__device__ __forceinline__ int halo_points(const int2* __restrict__ hash, int n_sorted, int H, int W, int k, int vb,
-                                           int rows, int u0, int c0 = 0, int c1 = kTileW) {
-  const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
-  const int rv0 = max(0, vb - lo), rv1 = min(H - 1, vb + rows - 1 + hi);
-  const int ru0 = max(0, u0 + c0 - lo), ru1 = min(W - 1, u0 + c1 - 1 + hi);
-  const int nu = ru1 - ru0 + 1, ncells = (rv1 - rv0 + 1) * nu;
-  int sum = 0;
-  for (int c = (threadIdx.x & 31); c < ncells; c += 32) {
-    const int2 rg = bucket_range(__ldg(hash + (size_t)(rv0 + c / nu) * W + ru0 + c % nu), n_sorted);
-    sum += min(rg.y - rg.x, kStageCap + 1);
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-  return sum;
-}
-
 // Items of tile t (local to its view) of an H x W image, appended to the queue.
 // The clipped point counts of the tile's whole window halo (up to 12 rows x
 // 36 columns) are loaded once, two columns per lane; the halo of any row band
 // or column range of the tile is a sub-rectangle of it, summed from those
 // registers with one warp reduction.
 __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k, int tiles_x,
-                                          int t, int view, Sched& sc) {
+                                          int t, int view, int cap, Sched& sc) {
   constexpr int kHaloRows = kTileH + kMaxKernel - 1;
   const int lane = threadIdx.x & 31;
   const int v0 = (t / tiles_x) * kTileH, u0 = (t % tiles_x) * kTileW;
@@ -1046,11 +1049,11 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
     if (vv <= hv1) {
       if (ua <= hu1) {
         const int2 rg = bucket_range(__ldg(hash + (size_t)vv * W + ua), n_sorted);
-        ca[h] = min(rg.y - rg.x, kStageCap + 1);
+        ca[h] = min(rg.y - rg.x, cap + 1);
       }
       if (ub <= hu1) {
         const int2 rg = bucket_range(__ldg(hash + (size_t)vv * W + ub), n_sorted);
-        cb[h] = min(rg.y - rg.x, kStageCap + 1);
+        cb[h] = min(rg.y - rg.x, cap + 1);
       }
     }
   }
@@ -1069,12 +1072,13 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     return sum;
   };
-  // split the tile's rows until each item's halo holds at most kSplitWork
-  // points (so no item runs much longer than the average) or is one row
+  // split the tile's rows until each item's halo holds at most `cap` points
+  // (the stage's capacity, so no item runs much longer than the average) or
+  // is one row
   for (int vb = v0; vb < v_end;) {
     int rows = v_end - vb;
     int sum = halo(vb, rows, 0, kTileW);
-    while (sum > kSplitWork && rows > 1) {
+    while (sum > cap && rows > 1) {
       rows = (rows + 1) >> 1;
       sum = halo(vb, rows, 0, kTileW);
     }
@@ -1084,7 +1088,7 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
       if (lane == 0) {
         const int c = (int)(((long long)min(hs, 1 << 24) * rows * kTileH * (c1 - c0)) /
                             ((long long)(rows + k - 1) * (c1 - c0 + k - 1)));
-        const int w = hs > kStageCap ? c * 4 : c;
+        const int w = hs > cap ? c * 4 : c;
         const int i = atomicAdd(sc.n_items, 1);
         sc.work[i] = w;
         sc.item[i] = (t << 8) | ((vb - v0) << 4) | rows;
@@ -1093,12 +1097,12 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
         atomicAdd(sc.counts + (sc.view ? view * 32 : 0) + cost_class(w), 1);
       }
     };
-    if (sum <= kStageCap) {
+    if (sum <= cap) {
       emit(sum, 0, kTileW);
     } else {  // one row: halves, then quarters, until the halo fits
       for (int c0 = 0; c0 < kTileW && u0 + c0 < W; c0 += kTileW / 2) {
         const int hs = halo(vb, rows, c0, c0 + kTileW / 2);
-        if (hs <= kStageCap) {
+        if (hs <= cap) {
           emit(hs, c0, c0 + kTileW / 2);
           continue;
         }
@@ -1111,10 +1115,10 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
 }
 
 __global__ void __launch_bounds__(256) k_tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k,
-                                                   int tiles_x, int ntiles, Sched sc) {
+                                                   int tiles_x, int ntiles, int cap, Sched sc) {
   const int t = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (t >= ntiles) return;
-  tile_work(hash, n_sorted, H, W, k, tiles_x, t, 0, sc);
+  tile_work(hash, n_sorted, H, W, k, tiles_x, t, 0, cap, sc);
 }
 
 __global__ void __launch_bounds__(256) k_tile_order(Sched sc) {
@@ -1174,8 +1178,9 @@ __global__ void __launch_bounds__(256) k_batch_order_place(Sched sc, const int* 
 
 // Rays of rows [v0, v0 + rows) and tile columns [c0, c1) of the tile at u0
 // (u0 + c0 < width).
-__device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int v0, int rows, int u0, int c0 = 0,
-                                             int c1 = kTileW) {
+template <int kCap>
+__device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<kCap>& st, int v0, int rows, int u0,
+                                             int c0 = 0, int c1 = kTileW) {
   const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
   const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
   const int rv0 = max(0, v0 - lo), rv1 = min(H - 1, v0 + rows - 1 + hi);
@@ -1195,7 +1200,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
       const int2 rg = bucket_range(__ldg(a.hash + (size_t)vv * W + uu), a.n_sorted);
       st.start[c] = rg.x;
       // capped so the prefix cannot overflow; a capped cell alone exceeds the stage
-      cnt[q] = min(rg.y - rg.x, kStageCap + 1);
+      cnt[q] = min(rg.y - rg.x, kCap + 1);
     }
     local += cnt[q];
   }
@@ -1221,7 +1226,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
   if (tid == 0) st.off[ncells] = total;
   __syncthreads();
 
-  const bool staged = total <= kStageCap;
+  const bool staged = total <= kCap;
   if (staged) {
     for (int i = tid; i < total; i += kThreads) {
       int lo_c = 0, hi_c = ncells;  // off[lo_c] <= i < off[hi_c]
@@ -1261,7 +1266,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
         for (int l = 0; l < k * k; l++) {
           int vv, uu;
           window_cell(pv, pu, k, H, W, l, vv, uu);
-          const int2 rg = staged ? SrcStaged{&st, rv0, ru0, nu}.range(a, vv, uu) : SrcGlobal{}.range(a, vv, uu);
+          const int2 rg = staged ? SrcStaged<kCap>{&st, rv0, ru0, nu}.range(a, vv, uu) : SrcGlobal{}.range(a, vv, uu);
           T += rg.y - rg.x;
         }
       }
@@ -1301,7 +1306,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
       if (rk < nvalid) {
         const int px = st.order[rk];
         if (staged)
-          sample_ray(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31), &st.kept[0][tid]);
+          sample_ray(a, SrcStaged<kCap>{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31), &st.kept[0][tid]);
         else
           sample_ray(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31), nullptr);
       }
@@ -1311,16 +1316,17 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage& st, int
     if (h >= nheavy) break;
     const int px = st.order[h];
     if (staged)
-      sample_ray_warp(a, SrcStaged{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
+      sample_ray_warp(a, SrcStaged<kCap>{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
     else
       sample_ray_warp(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
   }
   __syncthreads();  // the stage is reused by the next tile
 }
 
-__global__ void __launch_bounds__(kThreads, kBlocksPerSM) k_quick_sampling(SampleArgs a, Sched sc, int tiles_x) {
+template <class Cfg>
+__global__ void __launch_bounds__(kThreads, Cfg::kBlocks) k_quick_sampling(SampleArgs a, Sched sc, int tiles_x) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Stage& st = *reinterpret_cast<Stage*>(smem_raw);
+  Stage<Cfg::kCap>& st = *reinterpret_cast<Stage<Cfg::kCap>*>(smem_raw);
   __shared__ int s_next;
   const int n = *sc.n_items;
   for (;;) {
@@ -1439,7 +1445,7 @@ __global__ void k_batch_pack(const SampleArgs* __restrict__ args, const int* __r
 // One warp per global tile: find its view, then queue the tile's items.
 __global__ void __launch_bounds__(256) k_batch_tile_work(const SampleArgs* __restrict__ args,
                                                          const int* __restrict__ tile_base, int n_views,
-                                                         int total_tiles, Sched sc) {
+                                                         int total_tiles, int cap, Sched sc) {
   const int g = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (g >= total_tiles) return;
   int lo = 0, hi = n_views;  // tile_base[lo] <= g < tile_base[hi]
@@ -1452,14 +1458,16 @@ __global__ void __launch_bounds__(256) k_batch_tile_work(const SampleArgs* __res
   }
   const SampleArgs& a = args[lo];
   const int tiles_x = (a.cam.width + kTileW - 1) / kTileW;
-  tile_work(a.hash, a.n_sorted, a.cam.height, a.cam.width, a.opt.k, tiles_x, g - tile_base[lo], lo, sc);
+  tile_work(a.hash, a.n_sorted, a.cam.height, a.cam.width, a.opt.k, tiles_x, g - tile_base[lo], lo, cap, sc);
 }
 
 // The persistent sampling kernel over the batch's queue; each item's view
 // arguments are loaded into shared memory before the tile is processed.
-__global__ void __launch_bounds__(kThreads, kBlocksPerSM) k_quick_sampling_batch(const SampleArgs* __restrict__ args, Sched sc) {
+template <class Cfg>
+__global__ void __launch_bounds__(kThreads, Cfg::kBlocks)
+    k_quick_sampling_batch(const SampleArgs* __restrict__ args, Sched sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Stage& st = *reinterpret_cast<Stage*>(smem_raw);
+  Stage<Cfg::kCap>& st = *reinterpret_cast<Stage<Cfg::kCap>*>(smem_raw);
   __shared__ int s_next;
   __shared__ SampleArgs s_args;
   const int n = *sc.n_items;
@@ -1489,30 +1497,67 @@ __global__ void k_ray_directions(DevCamera cam, float* __restrict__ dirs) {
   dirs[3 * (size_t)p + 2] = r.d[2];
 }
 
-// The stage exceeds the 48 KB default of dynamic shared memory: opt the kernel
-// in once per device and size the persistent grid from its occupancy.
-int32_t sampling_grid(int* blocks, int* sm_count = nullptr) {
+// The sampling kernels of each stage configuration.
+struct SamplingKernels {
+  void (*view)(SampleArgs, Sched, int);
+  void (*batch)(const SampleArgs*, Sched);
+  size_t smem;
+  int cap;
+};
+template <class Cfg>
+static SamplingKernels sampling_kernels() {
+  return {k_quick_sampling<Cfg>, k_quick_sampling_batch<Cfg>, sizeof(Stage<Cfg::kCap>), Cfg::kCap};
+}
+static const SamplingKernels& stage_kernels(int config) {  // config 1..kStageConfigs
+  static const SamplingKernels table[kStageConfigs] = {sampling_kernels<Cfg2560x4>(), sampling_kernels<Cfg3712x3>(),
+                                                       sampling_kernels<Cfg5888x2>()};
+  return table[config - 1];
+}
+
+// The stage exceeds the 48 KB default of dynamic shared memory: opt the
+// configuration's kernels in once per device and size the persistent grid
+// from their occupancy.
+int32_t sampling_grid(int config, int* blocks, int* sm_count = nullptr) {
   static std::mutex mu;
-  static int grid[128] = {0}, sm_counts[128] = {0};
+  static int grid[128][kStageConfigs] = {{0}}, sm_counts[128] = {0};
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
-    return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaGetDevice failed");
+  if (cudaGetDevice(&dev) != cudaSuccess) return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaGetDevice failed");
+  if (dev < 0 || dev >= 128)
+    return set_error(HP_ERR_UNSUPPORTED, "hp_quick_sampling: device ordinal %d is beyond the 128 devices it tracks",
+                     dev);
   std::lock_guard<std::mutex> lock(mu);
-  if (!grid[dev]) {
-    cudaError_t e =
-        cudaFuncSetAttribute(k_quick_sampling, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Stage));
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_quick_sampling_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Stage));
+  int& g = grid[dev][config - 1];
+  if (!g) {
+    const SamplingKernels& K = stage_kernels(config);
+    cudaError_t e = cudaFuncSetAttribute(K.view, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(K.batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem);
     int sms = 0, per_sm = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_quick_sampling, kThreads, sizeof(Stage));
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, K.view, kThreads, K.smem);
     if (e != cudaSuccess) return set_error(HP_ERR_CUDA, "hp_quick_sampling: kernel set-up: %s", cudaGetErrorString(e));
-    grid[dev] = sms * (per_sm > 0 ? per_sm : 1);
+    g = sms * (per_sm > 0 ? per_sm : 1);
     sm_counts[dev] = sms;
   }
-  *blocks = grid[dev];
+  *blocks = g;
   if (sm_count) *sm_count = sm_counts[dev];
+  return HP_OK;
+}
+
+// Launch tuning shared by both entry points; outputs never depend on it.
+struct Tune {
+  int heavy = kHeavyWindow, per_sm = 0, config = 1;
+};
+
+static int32_t read_tuning(const char* who, const hp_tuning* tuning, Tune& t) {
+  if (!tuning) return HP_OK;
+  if (tuning->heavy_window < 0 || tuning->heavy_window > kMaxHeavyWindow || tuning->blocks_per_sm < 0 ||
+      tuning->stage_config < 0 || tuning->stage_config > kStageConfigs)
+    return set_error(HP_ERR_INVALID_ARGUMENT,
+                     "%s: tuning out of range (heavy_window 0..%d, blocks_per_sm >= 0, stage_config 0..%d)", who,
+                     kMaxHeavyWindow, kStageConfigs);
+  if (tuning->heavy_window > 0) t.heavy = tuning->heavy_window;
+  t.per_sm = tuning->blocks_per_sm;
+  if (tuning->stage_config > 0) t.config = tuning->stage_config;
   return HP_OK;
 }
 
@@ -1635,13 +1680,16 @@ static int32_t check_sampling(const char* who, const float* xyz, int64_t n_point
   return HP_OK;
 }
 
-extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const hp_camera* cam, const hp_options* opt,
-                                     const int32_t* sorted_point_idx, int64_t n_sorted, const int32_t* hash_table,
-                                     float* sp_xyz, int32_t* pc_idx, float* sp_t, uint8_t* mask, void* workspace,
-                                     size_t workspace_bytes, hp_stream_t stream) {
+extern "C" int32_t hp_quick_sampling_tuned(const float* xyz, int64_t n_points, const hp_camera* cam,
+                                           const hp_options* opt, const int32_t* sorted_point_idx, int64_t n_sorted,
+                                           const int32_t* hash_table, float* sp_xyz, int32_t* pc_idx, float* sp_t,
+                                           uint8_t* mask, const hp_tuning* tuning, void* workspace,
+                                           size_t workspace_bytes, hp_stream_t stream) {
   if (int32_t rc = check_sampling("hp_quick_sampling", xyz, n_points, cam, opt, sorted_point_idx, n_sorted, hash_table,
                                   sp_xyz, pc_idx, sp_t, mask))
     return rc;
+  Tune tn;
+  if (int32_t rc = read_tuning("hp_quick_sampling", tuning, tn)) return rc;
   const SchedLayout L = sched_layout(cam->height, cam->width, n_sorted);
   if (!workspace || workspace_bytes < L.total || ((uintptr_t)workspace & 255) != 0)
     return set_error(HP_ERR_WORKSPACE, "hp_quick_sampling: workspace needs %zu bytes, 256-byte aligned (got %zu)",
@@ -1659,9 +1707,11 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
   a.pc_idx = pc_idx;
   a.sp_t = sp_t;
   a.mask = mask;
-  a.heavy = kHeavyWindow;
-  int blocks = 0;
-  if (int32_t rc = sampling_grid(&blocks)) return rc;
+  a.heavy = tn.heavy;
+  int blocks = 0, sms = 0;
+  if (int32_t rc = sampling_grid(tn.config, &blocks, &sms)) return rc;
+  if (tn.per_sm > 0 && tn.per_sm * sms < blocks) blocks = tn.per_sm * sms;
+  const SamplingKernels& K = stage_kernels(tn.config);
   const int tiles_x = (cam->width + kTileW - 1) / kTileW;
   const int ntiles = tiles_x * ((cam->height + kTileH - 1) / kTileH);
   char* ws = (char*)workspace;
@@ -1684,14 +1734,22 @@ extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const h
     if (int32_t rc = check_launch("k_pack_points")) return rc;
   }
   k_tile_work<<<(ntiles + 7) / 8, 256, 0, st>>>(a.hash, a.n_sorted, cam->height, cam->width, opt->kernel_size, tiles_x,
-                                                 ntiles, sc);
+                                                 ntiles, K.cap, sc);
   if (int32_t rc = check_launch("k_tile_work")) return rc;
   k_tile_order<<<(ntiles + 255) / 256 < 148 ? (ntiles + 255) / 256 : 148, 256, 0, st>>>(sc);
   if (int32_t rc = check_launch("k_tile_order")) return rc;
   // a split tile yields up to kItemsPerTile items: size the persistent grid by those, not by tiles
   const int64_t max_items = (int64_t)ntiles * kItemsPerTile;
-  k_quick_sampling<<<blocks < max_items ? blocks : (int)max_items, kThreads, sizeof(Stage), st>>>(a, sc, tiles_x);
+  K.view<<<blocks < max_items ? blocks : (int)max_items, kThreads, K.smem, st>>>(a, sc, tiles_x);
   return check_launch("k_quick_sampling");
+}
+
+extern "C" int32_t hp_quick_sampling(const float* xyz, int64_t n_points, const hp_camera* cam, const hp_options* opt,
+                                     const int32_t* sorted_point_idx, int64_t n_sorted, const int32_t* hash_table,
+                                     float* sp_xyz, int32_t* pc_idx, float* sp_t, uint8_t* mask, void* workspace,
+                                     size_t workspace_bytes, hp_stream_t stream) {
+  return hp_quick_sampling_tuned(xyz, n_points, cam, opt, sorted_point_idx, n_sorted, hash_table, sp_xyz, pc_idx, sp_t,
+                                 mask, nullptr, workspace, workspace_bytes, stream);
 }
 
 // packed-point slots of a batch: each view's n_sorted rounded up to 16
@@ -1720,14 +1778,8 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
                                            hp_stream_t stream) {
   static const char* who = "hp_quick_sampling_batch";
   if (!views || n_views <= 0) return set_error(HP_ERR_INVALID_ARGUMENT, "%s: no views", who);
-  int heavy = kHeavyWindow, per_sm = 0;
-  if (tuning) {
-    if (tuning->heavy_window < 0 || tuning->heavy_window > kMaxHeavyWindow || tuning->blocks_per_sm < 0)
-      return set_error(HP_ERR_INVALID_ARGUMENT, "%s: tuning out of range (heavy_window 0..%d, blocks_per_sm >= 0)",
-                       who, kMaxHeavyWindow);
-    if (tuning->heavy_window > 0) heavy = tuning->heavy_window;
-    per_sm = tuning->blocks_per_sm;
-  }
+  Tune tn;
+  if (int32_t rc = read_tuning(who, tuning, tn)) return rc;
   for (int32_t v = 0; v < n_views; v++) {
     const hp_view& hv = views[v];
     if (int32_t rc = check_sampling(who, hv.xyz, hv.n_points, &hv.cam, &hv.opt, hv.sorted_point_idx, hv.n_sorted,
@@ -1746,8 +1798,9 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
     return set_error(HP_ERR_WORKSPACE, "%s: workspace needs %zu bytes, 256-byte aligned (got %zu)", who, B.total,
                      workspace_bytes);
   int blocks = 0, sms = 0;
-  if (int32_t rc = sampling_grid(&blocks, &sms)) return rc;
-  if (per_sm > 0 && per_sm * sms < blocks) blocks = per_sm * sms;
+  if (int32_t rc = sampling_grid(tn.config, &blocks, &sms)) return rc;
+  if (tn.per_sm > 0 && tn.per_sm * sms < blocks) blocks = tn.per_sm * sms;
+  const SamplingKernels& K = stage_kernels(tn.config);
   char* ws = (char*)workspace;
   cudaStream_t st = (cudaStream_t)stream;
   if (!views_device) {  // copy the table into the workspace
@@ -1774,21 +1827,21 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
       cudaMemsetAsync(ws + B.buckets, 0, 2 * bucket_bytes, st) != cudaSuccess)
     return set_error(HP_ERR_CUDA, "%s: memset failed", who);
   int* pack_base = (int*)(ws + B.pack_base);
-  k_batch_setup<<<1, 32, 0, st>>>(views_device, n_views, heavy, args, tile_base, pack_base, (float4*)(ws + B.pts));
+  k_batch_setup<<<1, 32, 0, st>>>(views_device, n_views, tn.heavy, args, tile_base, pack_base, (float4*)(ws + B.pts));
   if (int32_t rc = check_launch("k_batch_setup")) return rc;
   if (total_slots > 0) {
     k_batch_pack<<<(unsigned)((total_slots + 255) / 256), 256, 0, st>>>(args, pack_base, n_views, (int)total_slots);
     if (int32_t rc = check_launch("k_batch_pack")) return rc;
   }
   const int nt = (int)total_tiles;
-  k_batch_tile_work<<<(nt + 7) / 8, 256, 0, st>>>(args, tile_base, n_views, nt, sc);
+  k_batch_tile_work<<<(nt + 7) / 8, 256, 0, st>>>(args, tile_base, n_views, nt, K.cap, sc);
   if (int32_t rc = check_launch("k_batch_tile_work")) return rc;
   k_batch_order_scan<<<1, 1024, 0, st>>>(sc, n_views, base);
   if (int32_t rc = check_launch("k_batch_order_scan")) return rc;
   k_batch_order_place<<<(nt + 255) / 256 < 148 ? (nt + 255) / 256 : 148, 256, 0, st>>>(sc, base);
   if (int32_t rc = check_launch("k_batch_order_place")) return rc;
   const int64_t max_items = (int64_t)nt * kItemsPerTile;
-  k_quick_sampling_batch<<<blocks < max_items ? blocks : (int)max_items, kThreads, sizeof(Stage), st>>>(args, sc);
+  K.batch<<<blocks < max_items ? blocks : (int)max_items, kThreads, K.smem, st>>>(args, sc);
   return check_launch("k_quick_sampling_batch");
 }
 

@@ -1,8 +1,10 @@
-// Self-check of the tensor-core operand forms of hp_tc.cuh: one tcgen05.mma,
+// Self-check of the tensor-core operand forms of hp_tc.cuh (test library
+// only, include/hashpoint_b200_testing.h): one tcgen05.mma,
 // D [128, 256] fp32 = A [128 x 16] * B [256 x 16]^T (bf16), from operand
 // images the caller laid out as shared memory, with the descriptor of each
 // operand starting at a chosen byte offset into its image.  The tests compare
 // D with a host product for each form the Aggregator's kernels use.
+#include "../../include/hashpoint_b200_testing.h"
 #include "hp_common.cuh"
 #include "hp_tc.cuh"
 

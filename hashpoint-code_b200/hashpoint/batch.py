@@ -13,10 +13,12 @@ The whole batch can be captured once as a CUDA graph and replayed (`capture`,
 `replay`): buffers and the device view table are allocated up front and never
 move, and no call in the batch synchronises with the host.
 
-`Autotuner` picks the launch tuning of hp_quick_sampling_batch (which rays a
-whole warp serves, resident blocks per SM) by timing the candidates on the
-first batch of a shape class and caching the winner; outputs never depend on
-the choice.
+`Autotuner` picks the launch tuning of hp_quick_sampling_batch -- the stage
+configuration of the sampling pipeline (items in flight per block, staged
+points per item, blocks per SM; which items get split into row bands follows
+from the staged capacity) and which rays a whole warp serves -- by timing the
+candidates on the first batch of a shape class and caching the winner;
+outputs never depend on the choice.
 """
 import ctypes
 import math
@@ -88,7 +90,7 @@ class BatchRenderer:
             raise RuntimeError("BatchRenderer: invalid views")
         self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
         self.streams = [torch.cuda.Stream(self.device) for _ in range(max(1, int(build_streams)))]
-        self.tuning = native.HpTuning(0, 0)
+        self.tuning = ops.make_tuning()
         self.graph = None
 
     # -- work ---------------------------------------------------------------
@@ -183,8 +185,8 @@ class Autotuner:
     Candidates are timed with CUDA events on the renderer's own batch; the
     cache is filled once per class and then only read."""
 
-    HEAVY = (160, 224, 320)
-    BLOCKS = (0, 2)
+    HEAVY = (224, 320)
+    STAGES = native.STAGE_CONFIGS
 
     def __init__(self, reps=3):
         self.reps = int(reps)
@@ -210,19 +212,19 @@ class Autotuner:
         return best
 
     def tune(self, r):
-        """Set r.tuning to the cached or newly measured best; returns (heavy_window, blocks_per_sm)."""
+        """Set r.tuning to the cached or newly measured best; returns (stage_config, heavy_window)."""
         k = self.key(r)
         with self.lock:
             hit = self.cache.get(k)
         if hit is None:
             r.build()
             results = []
-            for h in self.HEAVY:
-                for b in self.BLOCKS:
-                    r.tuning = native.HpTuning(h, b)
-                    results.append((self._time(r), h, b))
-            _, h, b = min(results)
+            for c in self.STAGES:
+                for h in self.HEAVY:
+                    r.tuning = ops.make_tuning(heavy_window=h, stage_config=c)
+                    results.append((self._time(r), c, h))
+            _, c, h = min(results)
             with self.lock:
-                hit = self.cache.setdefault(k, (h, b))
-        r.tuning = native.HpTuning(*hit)
+                hit = self.cache.setdefault(k, (c, h))
+        r.tuning = ops.make_tuning(heavy_window=hit[1], stage_config=hit[0])
         return hit

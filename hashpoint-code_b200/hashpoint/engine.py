@@ -42,8 +42,9 @@ class CameraTable:
 class ViewPipeline:
     """pts2plane + quick_sampling for a fixed (N, H, W, S, P), buffers allocated once."""
 
-    def __init__(self, n_points, height, width, options, device, sort=False):
+    def __init__(self, n_points, height, width, options, device, sort=False, tuning=None):
         self.n, self.H, self.W = int(n_points), int(height), int(width)
+        self.tuning = tuning  # HpTuning of the sampling launch (None = defaults)
         self.opt = make_options(options)
         self.sort = int(bool(sort))
         self.device = torch.device(device)
@@ -70,12 +71,12 @@ class ViewPipeline:
         native.check(rc, "hp_pts2plane")
 
     def sample(self, xyz, cam, stream):
-        rc = native.lib().hp_quick_sampling(_vp(xyz.data_ptr()), self.n, ctypes.byref(cam), ctypes.byref(self.opt),
-                                            _vp(self.sidx.data_ptr()), self.n, _vp(self.hash.data_ptr()),
-                                            _vp(self.sp_xyz.data_ptr()), _vp(self.pc_idx.data_ptr()),
-                                            _vp(self.sp_t.data_ptr()), _vp(self.mask.data_ptr()),
-                                            _vp(self.ws_sample.data_ptr()), self.ws_sample_bytes,
-                                            _vp(stream.cuda_stream))
+        rc = native.lib().hp_quick_sampling_tuned(
+            _vp(xyz.data_ptr()), self.n, ctypes.byref(cam), ctypes.byref(self.opt), _vp(self.sidx.data_ptr()), self.n,
+            _vp(self.hash.data_ptr()), _vp(self.sp_xyz.data_ptr()), _vp(self.pc_idx.data_ptr()),
+            _vp(self.sp_t.data_ptr()), _vp(self.mask.data_ptr()),
+            ctypes.byref(self.tuning) if self.tuning is not None else None, _vp(self.ws_sample.data_ptr()),
+            self.ws_sample_bytes, _vp(stream.cuda_stream))
         native.check(rc, "hp_quick_sampling")
 
     def render(self, xyz, cam, stream=None):

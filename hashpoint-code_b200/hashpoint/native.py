@@ -12,7 +12,9 @@ device, and pass raw pointers plus torch's current CUDA stream.
 import ctypes
 import fcntl
 import os
+import shutil
 import subprocess
+import tempfile
 import threading
 from concurrent.futures import ThreadPoolExecutor
 
@@ -25,19 +27,26 @@ LIB_NAME = "libhashpoint_b200.so"
 LIB_PATH = os.path.join(LIB_DIR, LIB_NAME)
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
-SOURCES = ["hp_api.cu", "hp_build.cu", "hp_sample.cu", "hp_query.cu", "hp_feature.cu", "hp_aggregator.cu",
-           "hp_tc_check.cu"]
+SOURCES = ["hp_api.cu", "hp_build.cu", "hp_sample.cu", "hp_query.cu", "hp_feature.cu", "hp_aggregator.cu"]
+# The test-only library (include/hashpoint_b200_testing.h): the tensor-core operand-form self-check and a
+# wait-expiry test of the Aggregator, compiled with the sources they exercise; never loaded by the product.
+TESTING_LIB_NAME = "libhashpoint_b200_testing.so"
+TESTING_LIB_PATH = os.path.join(LIB_DIR, TESTING_LIB_NAME)
+TESTING_SOURCES = ["hp_api.cu", "hp_aggregator.cu", "hp_tc_check.cu"]
+TESTING_FLAGS = ["-DHP_TESTING"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 
 # C-ABI symbols declared in include/hashpoint_b200.h
 EXPORTS = ["hp_version", "hp_last_error", "hp_projection_rounding", "hp_pts2plane_workspace_size", "hp_pts2plane",
            "hp_pts2plane_noalloc", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling",
+           "hp_quick_sampling_tuned",
            "hp_quick_sampling_batch_workspace_size", "hp_quick_sampling_batch", "hp_quick_query_for_nearby_point",
            "hp_scatter", "hp_ray_directions", "hp_mask_scan", "hp_mask_scan_workspace_size", "hp_feature_query",
            "hp_clamp_t", "hp_render", "hp_aggregator_packed_size", "hp_aggregator_pack",
-           "hp_aggregator_workspace_size", "hp_aggregator_forward", "hp_aggregator_status",
-           "hp_tc_check_image_bytes", "hp_tc_check_mma"]
+           "hp_aggregator_workspace_size", "hp_aggregator_forward", "hp_aggregator_status"]
+# declared in include/hashpoint_b200_testing.h, exported by the test-only library
+TESTING_EXPORTS = ["hp_tc_check_image_bytes", "hp_tc_check_mma", "hp_aggregator_forward_withheld"]
 
 HP_OK = 0
 
@@ -46,47 +55,81 @@ class HashPointError(RuntimeError):
     pass
 
 
-def _sources():
-    return [os.path.join(CSRC, s) for s in SOURCES]
+def _sources(names=None):
+    return [os.path.join(CSRC, s) for s in (names or SOURCES)]
 
 
-def _deps():
-    deps = _sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    deps.append(os.path.join(INCLUDE, "hashpoint_b200.h"))
+def _deps(names=None):
+    deps = _sources(names) + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    deps += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
     return deps
 
 
-def needs_build():
-    if not os.path.exists(LIB_PATH):
+def needs_build(path=None, names=None):
+    path = path or LIB_PATH
+    if not os.path.exists(path):
         return True
-    t = os.path.getmtime(LIB_PATH)
-    return any(os.path.getmtime(d) > t for d in _deps())
+    t = os.path.getmtime(path)
+    return any(os.path.getmtime(d) > t for d in _deps(names))
 
 
 def build(force=False, verbose=False, extra_flags=()):
     """Compile the CUDA sources for sm_100a into the in-tree shared library.
 
-    Processes that build at once (the ranks of a torchrun job, test workers)
-    take turns on a lock file next to the library; each re-checks after taking
-    it, so the first one builds and the others find the library current."""
+    Every build compiles into a directory of its own and links to a file name
+    of its own, then renames the result over the library (atomic), so builders
+    that run at once -- the ranks of a torchrun job, test workers -- never
+    read or delete each other's files.  A lock file next to the library only
+    saves duplicate work: each builder re-checks after taking it, so the first
+    one builds and the others find the library current.  On a filesystem
+    without locks they simply all build."""
     if not force and not needs_build():
         return LIB_PATH
     os.makedirs(LIB_DIR, exist_ok=True)
     with open(os.path.join(LIB_DIR, ".build.lock"), "w") as lock:
         try:
             fcntl.flock(lock, fcntl.LOCK_EX)
-        except OSError:  # a filesystem without locks: build unserialised, as before
-            return _build_locked(verbose, extra_flags)
+        except OSError:  # a filesystem without locks: private build directories keep builders apart
+            return _build_private(verbose, extra_flags)
         try:
             if not force and not needs_build():
                 return LIB_PATH
-            return _build_locked(verbose, extra_flags)
+            return _build_private(verbose, extra_flags)
         finally:
             fcntl.flock(lock, fcntl.LOCK_UN)
 
 
-def _build_locked(verbose, extra_flags):
-    objs = [os.path.join(LIB_DIR, os.path.basename(s) + ".o") for s in _sources()]
+def build_testing(force=False, verbose=False):
+    """Compile the test-only library (TESTING_SOURCES with -DHP_TESTING) beside the product library,
+    under the same lock and private-directory protocol as build()."""
+    if not force and not needs_build(TESTING_LIB_PATH, TESTING_SOURCES):
+        return TESTING_LIB_PATH
+    os.makedirs(LIB_DIR, exist_ok=True)
+    with open(os.path.join(LIB_DIR, ".build.lock"), "w") as lock:
+        try:
+            fcntl.flock(lock, fcntl.LOCK_EX)
+        except OSError:
+            return _build_private(verbose, TESTING_FLAGS, TESTING_SOURCES, TESTING_LIB_PATH)
+        try:
+            if not force and not needs_build(TESTING_LIB_PATH, TESTING_SOURCES):
+                return TESTING_LIB_PATH
+            return _build_private(verbose, TESTING_FLAGS, TESTING_SOURCES, TESTING_LIB_PATH)
+        finally:
+            fcntl.flock(lock, fcntl.LOCK_UN)
+
+
+def _build_private(verbose, extra_flags, names=None, path=None):
+    work = tempfile.mkdtemp(prefix=".build-", dir=LIB_DIR)
+    try:
+        return _compile_and_link(work, verbose, extra_flags, names, path or LIB_PATH)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def _compile_and_link(work, verbose, extra_flags, names=None, path=None):
+    path = path or LIB_PATH
+    srcs = _sources(names)
+    objs = [os.path.join(work, os.path.basename(s) + ".o") for s in srcs]
 
     def compile_one(pair):
         src, obj = pair
@@ -97,18 +140,16 @@ def _build_locked(verbose, extra_flags):
         return p.stdout
 
     with ThreadPoolExecutor(max_workers=len(objs)) as ex:
-        outs = list(ex.map(compile_one, zip(_sources(), objs)))
-    tmp = LIB_PATH + ".tmp"
+        outs = list(ex.map(compile_one, zip(srcs, objs)))
+    tmp = os.path.join(work, os.path.basename(path))
     p = subprocess.run([NVCC, "-shared", "-o", tmp] + objs + ["-gencode", "arch=compute_100a,code=sm_100a"],
                        stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
     if p.returncode != 0:
         raise HashPointError("link failed:\n%s" % p.stdout)
-    os.replace(tmp, LIB_PATH)
-    for o in objs:
-        os.remove(o)
+    os.replace(tmp, path)
     if verbose:
         print("".join(outs))
-    return LIB_PATH
+    return path
 
 
 # ----------------------------------------------------------------------------
@@ -138,8 +179,11 @@ class HpAggregatorWeights(ctypes.Structure):
 
 
 class HpTuning(ctypes.Structure):
-    """Launch tuning of hp_quick_sampling_batch (0 = default)."""
-    _fields_ = [("heavy_window", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32)]
+    """Launch tuning of hp_quick_sampling_tuned / _batch (0 = default; see include/hashpoint_b200.h)."""
+    _fields_ = [("heavy_window", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("stage_config", ctypes.c_int32)]
+
+
+STAGE_CONFIGS = (1, 2, 3)  # hp_tuning.stage_config values
 
 
 class HpView(ctypes.Structure):
@@ -184,6 +228,9 @@ def lib():
         L.hp_quick_sampling_workspace_size.restype = sz
         L.hp_quick_sampling.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, vp, vp, vp, vp, sz, vp]
         L.hp_quick_sampling.restype = i32
+        L.hp_quick_sampling_tuned.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, vp, vp, vp,
+                                              ctypes.POINTER(HpTuning), vp, sz, vp]
+        L.hp_quick_sampling_tuned.restype = i32
         view_p = ctypes.POINTER(HpView)
         L.hp_quick_sampling_batch_workspace_size.argtypes = [view_p, i32]
         L.hp_quick_sampling_batch_workspace_size.restype = sz
@@ -211,10 +258,6 @@ def lib():
         L.hp_aggregator_forward.restype = i32
         L.hp_aggregator_status.argtypes = [vp, i64, vp]
         L.hp_aggregator_status.restype = i32
-        L.hp_tc_check_image_bytes.argtypes = [i32]
-        L.hp_tc_check_image_bytes.restype = sz
-        L.hp_tc_check_mma.argtypes = [vp, vp, i32, ctypes.c_uint32, i32, ctypes.c_uint32, vp, vp]
-        L.hp_tc_check_mma.restype = i32
         L.hp_quick_query_for_nearby_point.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, i64, vp, vp]
         L.hp_quick_query_for_nearby_point.restype = i32
         L.hp_scatter.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp]
@@ -225,9 +268,41 @@ def lib():
         return _lib
 
 
-def check(rc, what):
+_testing = None
+
+
+def testing_lib():
+    """Load the test-only library (raises HashPointError if it is missing)."""
+    global _testing
+    with _lock:
+        if _testing is not None:
+            return _testing
+        if not os.path.exists(TESTING_LIB_PATH):
+            raise HashPointError("test library %s is missing: build it with hashpoint.native.build_testing()"
+                                 % TESTING_LIB_PATH)
+        T = ctypes.CDLL(TESTING_LIB_PATH)
+        vp, i32, i64, sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t
+        T.hp_last_error.restype = ctypes.c_char_p
+        T.hp_tc_check_image_bytes.argtypes = [i32]
+        T.hp_tc_check_image_bytes.restype = sz
+        T.hp_tc_check_mma.argtypes = [vp, vp, i32, ctypes.c_uint32, i32, ctypes.c_uint32, vp, vp]
+        T.hp_tc_check_mma.restype = i32
+        T.hp_aggregator_workspace_size.argtypes = [i64]
+        T.hp_aggregator_workspace_size.restype = sz
+        T.hp_aggregator_status.argtypes = [vp, i64, vp]
+        T.hp_aggregator_status.restype = i32
+        T.hp_aggregator_forward_withheld.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp, vp, i64, i32, vp, vp, i64, vp,
+                                                     vp, vp, sz, i32, vp]
+        T.hp_aggregator_forward_withheld.restype = i32
+        _testing = T
+        return _testing
+
+
+def check(rc, what, L=None):
+    """Raise HashPointError with the library's message when rc is not HP_OK (L: the library that
+    made the call, default the product library)."""
     if rc != HP_OK:
-        msg = lib().hp_last_error().decode(errors="replace")
+        msg = (L or lib()).hp_last_error().decode(errors="replace")
         raise HashPointError("%s failed (%d): %s" % (what, rc, msg))
 
 

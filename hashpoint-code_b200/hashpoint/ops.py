@@ -119,8 +119,15 @@ def _hash_view(hash_table, height, width):
     return hash_table
 
 
-def quick_sampling(xyz, c2w, fx, fy, cx, cy, width, height, opt, sorted_point_idx, hash_table):
-    """(sp_xyz f32[H,W,S,3], pc_idx i32[H,W,S,P], sp_t f32[H,W,S], mask bool[H,W,S])."""
+def make_tuning(heavy_window=0, blocks_per_sm=0, stage_config=0):
+    """HpTuning for the sampling launches (0 = default for every field)."""
+    return native.HpTuning(int(heavy_window), int(blocks_per_sm), int(stage_config))
+
+
+def quick_sampling(xyz, c2w, fx, fy, cx, cy, width, height, opt, sorted_point_idx, hash_table, tuning=None):
+    """(sp_xyz f32[H,W,S,3], pc_idx i32[H,W,S,P], sp_t f32[H,W,S], mask bool[H,W,S]).
+
+    tuning: optional HpTuning (make_tuning); outputs do not depend on it."""
     check_input(xyz, "xyz_data", torch.float32)
     check_matrix(c2w, "c2w")
     check_input(sorted_point_idx, "sorted_point_idx_list", torch.int32)
@@ -137,9 +144,11 @@ def quick_sampling(xyz, c2w, fx, fy, cx, cy, width, height, opt, sorted_point_id
     L = native.lib()
     ws_bytes = L.hp_quick_sampling_workspace_size(sorted_point_idx.numel(), H, W)
     ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
-    rc = L.hp_quick_sampling(_ptr(xyz), xyz.shape[0], ctypes.byref(cam), ctypes.byref(o), _ptr(sorted_point_idx),
-                             sorted_point_idx.numel(), _ptr(hash_table), _ptr(sp_xyz), _ptr(pc_idx), _ptr(sp_t),
-                             _ptr(mask), _ptr(ws), ws_bytes, _stream(dev))
+    rc = L.hp_quick_sampling_tuned(_ptr(xyz), xyz.shape[0], ctypes.byref(cam), ctypes.byref(o),
+                                   _ptr(sorted_point_idx), sorted_point_idx.numel(), _ptr(hash_table), _ptr(sp_xyz),
+                                   _ptr(pc_idx), _ptr(sp_t), _ptr(mask),
+                                   ctypes.byref(tuning) if tuning is not None else None, _ptr(ws), ws_bytes,
+                                   _stream(dev))
     native.check(rc, "hp_quick_sampling")
     return sp_xyz, pc_idx, sp_t, mask
 
@@ -178,12 +187,13 @@ def batch_workspace_size(views):
     return native.lib().hp_quick_sampling_batch_workspace_size((native.HpView * n)(*views), n)
 
 
-def quick_sampling_batch(views, device, views_device=None, workspace=None, heavy_window=0, blocks_per_sm=0):
+def quick_sampling_batch(views, device, views_device=None, workspace=None, heavy_window=0, blocks_per_sm=0,
+                         stage_config=0):
     """hp_quick_sampling_batch over a list of HpView (see make_view); outputs are the views' own tensors.
 
     views_device: optional uint8 CUDA tensor holding the same table (for CUDA-graph capture).
     workspace: optional uint8 CUDA tensor of at least batch_workspace_size(views) bytes.
-    heavy_window, blocks_per_sm: launch tuning (0 = default); outputs do not depend on it."""
+    heavy_window, blocks_per_sm, stage_config: launch tuning (0 = default); outputs do not depend on it."""
     L = native.lib()
     n = len(views)
     table = (native.HpView * n)(*views)
@@ -192,7 +202,7 @@ def quick_sampling_batch(views, device, views_device=None, workspace=None, heavy
         raise RuntimeError("hp_quick_sampling_batch: invalid views")
     if workspace is None:
         workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=device)
-    tuning = native.HpTuning(int(heavy_window), int(blocks_per_sm))
+    tuning = make_tuning(heavy_window, blocks_per_sm, stage_config)
     rc = L.hp_quick_sampling_batch(table, _ptr(views_device), n, ctypes.byref(tuning), _ptr(workspace),
                                    workspace.numel(), _stream(torch.device(device)))
     native.check(rc, "hp_quick_sampling_batch")

@@ -171,7 +171,7 @@ class Server:
     on_result(request): called with each finished request (outputs attached)
     before its outputs are released."""
 
-    def __init__(self, store, budget_bytes, streams=3, max_views=16, on_result=None, tuning=(0, 0)):
+    def __init__(self, store, budget_bytes, streams=3, max_views=16, on_result=None, tuning=None):
         self.store = store
         self.budget = int(budget_bytes)
         self.max_views = int(max_views)
@@ -179,7 +179,7 @@ class Server:
         self.device = store.device
         self.streams = [torch.cuda.Stream(self.device) for _ in range(max(1, int(streams)))]
         self.free_slots = list(range(len(self.streams)))
-        self.tuning = native.HpTuning(*tuning)
+        self.tuning = tuning if tuning is not None else ops.make_tuning()
         self.out_bytes = 0
         self.batches = 0
 

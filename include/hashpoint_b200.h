@@ -105,11 +105,14 @@ HP_API int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_camera*
  * its scratch is an array built into the library (about 10 MB of device
  * memory on every GPU that loads the library, held until the process exits),
  * so it accepts at most HP_NOALLOC_MAX_POINTS points and HP_NOALLOC_MAX_PIXELS
- * pixels and returns HP_ERR_INVALID_ARGUMENT beyond that.  The first call on a
- * device looks up that device's address of the array (make it before any
- * stream capture).  All calls share the one array, so calls that overlap on
- * the GPU (on different streams, or from different threads) race: serialise
- * them.  Each call clears the parts of the array that must start at zero.
+ * pixels and returns HP_ERR_INVALID_ARGUMENT beyond that.  A call looks up its
+ * device's address of the array unless its stream is being captured; a
+ * captured call uses the address the device's last uncaptured call found, so
+ * make one call outside capture first (a captured call with none before it
+ * fails with HP_ERR_CUDA).  All calls share the one array, so calls that
+ * overlap on the GPU (on different streams, or from different threads) race:
+ * serialise them.  Each call clears the parts of the array that must start at
+ * zero.
  * No counterpart in the reference. */
 #define HP_NOALLOC_MAX_POINTS 262144
 #define HP_NOALLOC_MAX_PIXELS 1048576
@@ -232,15 +235,30 @@ HP_API int32_t hp_aggregator_status(const void* workspace, int64_t n_samples, hp
  * workspace must be 256-byte aligned. */
 HP_API size_t hp_quick_sampling_workspace_size(int64_t n_sorted, int32_t height, int32_t width);
 
-/* Launch tuning of hp_quick_sampling_batch (NULL or 0 fields = defaults).
- * Outputs never depend on it.  heavy_window: rays whose window holds more
- * candidates are served by a whole warp instead of one thread (0..4096;
- * default 320).  blocks_per_sm: resident blocks of the persistent sampling
- * kernel per SM (default: as many as fit). */
+/* Launch tuning of hp_quick_sampling_tuned and hp_quick_sampling_batch (NULL
+ * or 0 fields = defaults).  Outputs never depend on it.
+ *   heavy_window   rays whose window holds more candidates are served by a
+ *                  whole warp instead of one thread (0..4096; default 320).
+ *   blocks_per_sm  resident blocks of the persistent sampling kernel per SM
+ *                  (default: as many as fit).
+ *   stage_config   shared-memory stage of the sampling kernel (0 = 1):
+ *                  1: 2560 staged points per tile, 4 blocks per SM;
+ *                  2: 3712 points, 3 blocks per SM;  3: 5888 points, 2 blocks.
+ *                  Tiles whose window halo holds more points are split into
+ *                  row bands and column ranges, or read from global memory. */
 typedef struct hp_tuning {
   int32_t heavy_window;
   int32_t blocks_per_sm;
+  int32_t stage_config;
 } hp_tuning;
+
+/* hp_quick_sampling with launch tuning (see hp_tuning; NULL = defaults).
+ * No counterpart in the reference. */
+HP_API int32_t hp_quick_sampling_tuned(const float* xyz, int64_t n_points, const hp_camera* cam,
+                                       const hp_options* opt, const int32_t* sorted_point_idx, int64_t n_sorted,
+                                       const int32_t* hash_table, float* sp_xyz, int32_t* pc_idx, float* sp_t,
+                                       uint8_t* mask, const hp_tuning* tuning, void* workspace,
+                                       size_t workspace_bytes, hp_stream_t stream);
 
 /* One view of a batched hp_quick_sampling: the arguments of hp_quick_sampling
  * for that view (cloud, camera, options, its hash table and its outputs). */
@@ -300,26 +318,6 @@ HP_API int32_t hp_scatter(const int32_t* point_idx, const int32_t* point2img, co
 /* Normalised world-space direction of every pixel's ray, [H*W, 3], exactly as
  * the sampling kernels compute it (cam2world_ray, cuda_util.cuh:338-354). */
 HP_API int32_t hp_ray_directions(const hp_camera* cam, float* dirs, hp_stream_t stream);
-
-/* Diagnostics: a self-check of the tensor-core operand forms the Aggregator's
- * kernels use (no counterpart in the reference).  hp_tc_check_mma runs one
- * tcgen05.mma, d [128, 256] f32 = A [128 x 16] * B [256 x 16]^T in bf16, from
- * device images of shared memory (A: hp_tc_check_image_bytes(0) bytes, B:
- * hp_tc_check_image_bytes(1); 16-byte aligned).  The descriptor of each
- * operand starts a_offset / b_offset bytes into its image, in one of three
- * K-major forms:
- *   HP_TC_PLAIN  no swizzle: 8-row x 16-byte core matrices, K-adjacent ones
- *                128 bytes apart, 8-row groups 256 bytes apart;
- *   HP_TC_SW128  128-byte swizzle: a 128-byte row per matrix row, its 16-byte
- *                chunks permuted by chunk ^ (row % 8), 8-row atoms of 1024 bytes;
- *   HP_TC_SW64   64-byte swizzle: a 64-byte row per matrix row, chunks permuted
- *                by chunk ^ ((row / 2) % 4), 8-row atoms of 512 bytes.
- * Unlike the other entry points it allocates (a 4-byte status word) and
- * synchronises on stream. */
-enum { HP_TC_PLAIN = 0, HP_TC_SW128 = 1, HP_TC_SW64 = 2 };
-HP_API size_t hp_tc_check_image_bytes(int32_t operand);
-HP_API int32_t hp_tc_check_mma(const void* a_image, const void* b_image, int32_t a_form, uint32_t a_offset,
-                               int32_t b_form, uint32_t b_offset, float* d, hp_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -1,7 +1,8 @@
 """Build recipe for the reference's own CUDA extension, used only as a test checker.
 
 This script compiles the reference's `epcq/csrc` sources *where they lie* under
-the read-only reference checkout (default `/root/reference`) with plain
+the read-only reference checkout (the HP_REFERENCE_ROOT environment variable,
+else `/root/reference`) with plain
 `nvcc`/`g++` invocations (it does not run the reference's setup.py), for
 sm_100a, and links them into `oracle/_ref/epcq_ref_csrc.so`, a CPython
 extension module named `epcq_ref_csrc` that exposes the same pybind surface as
@@ -18,7 +19,7 @@ setup.py (setup.py:38-49 adds only the include dir), plus the sm_100a gencode.
 The output directory is git-ignored; the built .so travels with the repository
 snapshot to GPU machines, where the reference checkout itself is absent.
 
-Usage:  python oracle/build_ref.py [--ref /root/reference] [--force]
+Usage:  python oracle/build_ref.py [--ref REFERENCE_ROOT] [--force]
 """
 import argparse
 import os
@@ -34,6 +35,11 @@ SO_PATH = os.path.join(OUT_DIR, MODULE + ".so")
 
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+
+
+def default_root():
+    """Location of the reference checkout: $HP_REFERENCE_ROOT, else where this build reads it."""
+    return os.environ.get("HP_REFERENCE_ROOT", "/root/reference")
 
 
 def _torch_paths():
@@ -53,12 +59,13 @@ def _run(cmd):
     return proc.stdout
 
 
-def build(ref_root="/root/reference", force=False, verbose=True):
+def build(ref_root=None, force=False, verbose=True):
     """Compile the reference extension into oracle/_ref; return the .so path.
 
     Skips the build when the .so is newer than every source (unless force).
     Raises FileNotFoundError when the reference checkout is absent.
     """
+    ref_root = ref_root or default_root()
     csrc = os.path.join(ref_root, "epcq", "csrc")
     if not os.path.isdir(csrc):
         raise FileNotFoundError("reference sources not found at %s" % csrc)
@@ -115,7 +122,7 @@ def load():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference checkout (default: $HP_REFERENCE_ROOT or the build's)")
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     try:

@@ -42,10 +42,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "hashpoint-code_b200"))
 
 from hashpoint import synth  # noqa: E402
-
-OPT_FIELDS = ["kernel_size", "t_intvl", "radius_threshold", "sigma_threshold", "background_brightness",
-              "stop_threshold", "num_sample_points_per_ray", "num_point_cloud_per_sp", "num_point_per_ray",
-              "sdf2weight_gaussian_alpha", "sdf2weight_gaussian_gamma", "topK"]
+from ref_pipeline import OPT_FIELDS, RefPipeline  # noqa: E402,F401  (RefPipeline: used by the parity tests too)
 
 
 def plane_cloud(rng, n, cam, depth=2.0, jitter=0.0):
@@ -113,60 +110,6 @@ def build_cases():
                                         num_point_cloud_per_sp=8),
                       query=dict(n_rays=96, num_point_per_ray=[256, 8])))
     return cases
-
-
-class RefPipeline:
-    """The reference's Python-side steps, restated over torch, feeding the reference _C."""
-
-    def __init__(self, mod, dev):
-        self.C = mod
-        self.dev = dev
-
-    def camera_spec(self, c2w, w2c, cam):
-        s = self.C.CameraSpec()
-        s.c2w, s.w2c = c2w, w2c
-        s.fx, s.fy, s.cx, s.cy = cam.fx, cam.fy, cam.cx, cam.cy
-        s.width, s.height = cam.width, cam.height
-        return s
-
-    def options_spec(self, opt):
-        o = self.C.RenderOptions()
-        for f in OPT_FIELDS:
-            setattr(o, f, getattr(opt, f))
-        return o
-
-    def project(self, xyz, w2c, K, H, W):
-        pts_c = (w2c[:3, :3] @ xyz.t() + w2c[:3, 3:4]).t()
-        depth = pts_c[:, 2:3]
-        scrn = K @ pts_c.t()
-        scrn = scrn / scrn[2:3, :]
-        sx, sy = scrn[0, :], scrn[1, :]
-        sxi, syi = sx.to(torch.int32), sy.to(torch.int32)
-        pid = sxi + syi * W
-        inb = (0 <= sxi) & (sxi < W) & (0 <= syi) & (syi < H)
-        pid = torch.where(inb, pid, torch.full_like(pid, H * W))
-        return pid, depth.squeeze(1), sx, sy, pts_c
-
-    def sort(self, pid, depth):
-        n = pid.shape[0]
-        point_idx = torch.arange(n, dtype=torch.int32, device=pid.device)
-        pid_s, perm = torch.sort(pid.squeeze(), dim=-1, descending=False)
-        return pid_s, perm, depth[perm], point_idx[perm]
-
-    def scatter_hashtable(self, idx_s, pid_s, depth_s, H, W, sort):
-        n = pid_s.shape[0]
-        pad = torch.empty(n + 1, dtype=torch.int32, device=pid_s.device)
-        pad[:n] = pid_s
-        pad[n] = -7          # sentinel: stops the bucket walk at index n
-        return self.C.scatter_hashtable(idx_s, pad[:n], depth_s, [H, W], sort)
-
-    def scatter(self, idx_s, pid_s, depth_s, H, W, bins):
-        n = pid_s.shape[0]
-        pad = torch.empty(n + 1, dtype=torch.int32, device=pid_s.device)
-        pad[:n] = pid_s
-        pad[n] = -7
-        assert bool((depth_s[pid_s < H * W] >= 0).all())
-        return self.C.scatter(idx_s, pad[:n], depth_s, [H, W], bins)
 
 
 def run_case(rp, case, dev):

@@ -1,4 +1,6 @@
-"""The C-ABI library loads and exports every symbol include/hashpoint_b200.h declares.
+"""The C-ABI libraries load and export every symbol their headers declare:
+include/hashpoint_b200.h (the product library) and include/hashpoint_b200_testing.h
+(the test-only library).
 
 No compute is launched here: argument validation runs on the host and returns
 before any CUDA call, so these checks need no GPU.
@@ -11,11 +13,13 @@ import pytest
 
 from hashpoint import native
 
-HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "hashpoint_b200.h")
+INCLUDE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+HEADER = os.path.join(INCLUDE, "hashpoint_b200.h")
+TESTING_HEADER = os.path.join(INCLUDE, "hashpoint_b200_testing.h")
 
 
-def declared_symbols():
-    text = open(HEADER).read()
+def declared_symbols(header=HEADER):
+    text = open(header).read()
     return sorted(set(re.findall(r"HP_API\s+[\w\s\*]+?\b(hp_\w+)\s*\(", text)))
 
 
@@ -25,15 +29,29 @@ def L():
     return native.lib()
 
 
+@pytest.fixture(scope="module")
+def T():
+    native.build_testing()
+    return native.testing_lib()
+
+
 def test_header_declares_entry_points():
     syms = declared_symbols()
     assert "hp_quick_sampling" in syms and "hp_pts2plane" in syms
     assert set(syms) == set(native.EXPORTS)
+    assert set(declared_symbols(TESTING_HEADER)) == set(native.TESTING_EXPORTS)
 
 
 def test_library_exports_every_declared_symbol(L):
     for s in declared_symbols():
         assert hasattr(L, s), s
+
+
+def test_testing_library_exports_its_symbols_and_the_product_keeps_them_out(L, T):
+    for s in declared_symbols(TESTING_HEADER):
+        assert hasattr(T, s), s
+        with pytest.raises(AttributeError):
+            getattr(L, s)
 
 
 def test_version(L):
@@ -137,14 +155,15 @@ def test_batch_workspace_and_validation(L):
     assert L.hp_quick_sampling_batch_workspace_size(two, 0) == 0
     assert L.hp_quick_sampling_batch_workspace_size((native.HpView * 1)(_view(w=0)), 1) == 0
     ws = ctypes.c_void_p(0x100000)
-    t = native.HpTuning(0, 0)
+    t = native.HpTuning()
     bad = (native.HpView * 2)(_view(), _view(k=9))
     assert L.hp_quick_sampling_batch(bad, None, 2, ctypes.byref(t), ws, 1 << 30, None) == -1
     assert "view 1" in _err(L) and "kernel_size" in _err(L)
     assert L.hp_quick_sampling_batch(two, None, 0, ctypes.byref(t), ws, 1 << 30, None) == -1
     assert L.hp_quick_sampling_batch(two, None, 2, ctypes.byref(t), ws, b - 1, None) == -2
-    assert L.hp_quick_sampling_batch(two, None, 2, ctypes.byref(native.HpTuning(4097, 0)), ws, b, None) == -1
-    assert "tuning" in _err(L)
+    for bad_t in (native.HpTuning(4097), native.HpTuning(0, -1), native.HpTuning(0, 0, 4), native.HpTuning(0, 0, -1)):
+        assert L.hp_quick_sampling_batch(two, None, 2, ctypes.byref(bad_t), ws, b, None) == -1
+        assert "tuning" in _err(L)
 
 
 def test_pts2plane_checks_workspace(L):
@@ -202,8 +221,9 @@ def test_aggregator_sizes_and_validation(L):
     assert L.hp_aggregator_pack(ctypes.byref(w), p, packed, None) == -1 and "layer 0" in _err(L)
 
 
-def test_tc_check_validation(L):
+def test_tc_check_validation(T):
     """The operand-form self-check's argument checks, which run before any device work."""
+    L = T
     assert L.hp_tc_check_image_bytes(0) == 81920 and L.hp_tc_check_image_bytes(1) == 32768
     p = ctypes.c_void_p(0x100000)
     PLAIN, SW128, SW64 = 0, 1, 2

@@ -1,10 +1,12 @@
 """native.build() under concurrent processes: a builder waits for the lock
 another holds, then re-checks and does not rebuild a library that became
-current meanwhile.  The compile itself is stubbed out: no nvcc runs here."""
+current meanwhile; builders without a lock work in private directories.  The
+compiler itself is stubbed out: no nvcc runs here."""
 import fcntl
 import os
 import subprocess
 import sys
+import threading
 import time
 
 from hashpoint import native
@@ -20,7 +22,7 @@ def needs_build():
 def build_locked(verbose, extra_flags):
     raise SystemExit("rebuilt a current library")
 native.needs_build = needs_build
-native._build_locked = build_locked
+native._build_private = build_locked
 print(native.build() == native.LIB_PATH, len(calls), "%.6f" % calls[-1])
 """
 
@@ -51,5 +53,48 @@ def test_builds_without_a_lock_where_the_filesystem_has_none(monkeypatch):
 
     monkeypatch.setattr(native.fcntl, "flock", no_locks)
     monkeypatch.setattr(native, "needs_build", lambda: True)
-    monkeypatch.setattr(native, "_build_locked", lambda verbose, extra: calls.append(1) or native.LIB_PATH)
+    monkeypatch.setattr(native, "_build_private", lambda verbose, extra: calls.append(1) or native.LIB_PATH)
     assert native.build() == native.LIB_PATH and calls == [1]
+
+
+def test_unlocked_builders_at_once_keep_their_files_apart(monkeypatch, tmp_path):
+    """Two builders with no lock between them: each compiles and links in its own directory, so
+    neither links or deletes the other's objects, and the library ends up whole."""
+    lib = tmp_path / native.LIB_NAME
+    monkeypatch.setattr(native, "LIB_DIR", str(tmp_path))
+    monkeypatch.setattr(native, "LIB_PATH", str(lib))
+    seen = []
+
+    class Done:
+        returncode, stdout = 0, ""
+
+    def fake_run(cmd, **kw):
+        out = cmd[cmd.index("-o") + 1]
+        seen.append(os.path.dirname(out))
+        if "-shared" in cmd:  # the link reads every object of its own build
+            for o in cmd[cmd.index("-o") + 2:]:
+                if o.endswith(".o"):
+                    assert open(o).read() == "obj:" + os.path.dirname(out)
+        time.sleep(0.05)
+        with open(out, "w") as f:
+            f.write("obj:" + os.path.dirname(out) if out.endswith(".o") else "library")
+        return Done()
+
+    monkeypatch.setattr(native.subprocess, "run", fake_run)
+    errors = []
+
+    def builder():
+        try:
+            assert native._build_private(False, ()) == str(lib)
+        except Exception as e:  # noqa: BLE001 -- reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=builder) for _ in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(60)
+    assert not errors, errors
+    assert lib.read_text() == "library"
+    assert len(set(seen)) == 2  # two private directories
+    assert not [p for p in os.listdir(tmp_path) if p.startswith(".build-")]  # both cleaned up

@@ -104,8 +104,10 @@ def test_tuning_does_not_change_outputs():
     r.run()
     torch.cuda.synchronize()
     first = [tuple(t.clone() for t in r.outputs(i)) for i in range(len(r.views))]
-    for heavy, blocks in [(1, 0), (64, 1), (160, 2), (320, 3)]:
-        r.tuning = native.HpTuning(heavy, blocks)
+    cases = [(1, 0, 1), (64, 1, 2), (160, 2, 3), (320, 3, 1), (224, 0, 2), (4096, 0, 3)]
+    cases += [(320, 0, c) for c in native.STAGE_CONFIGS]
+    for heavy, blocks, stage in cases:
+        r.tuning = ops.make_tuning(heavy_window=heavy, blocks_per_sm=blocks, stage_config=stage)
         r.sample()
         torch.cuda.synchronize()
         for i in range(len(r.views)):
@@ -116,7 +118,7 @@ def test_autotuner_caches_per_shape_class():
     r, _ = _mixed_renderer(seed=9)
     tuner = batch.Autotuner(reps=1)
     choice = tuner.tune(r)
-    assert choice[0] in batch.Autotuner.HEAVY and choice[1] in batch.Autotuner.BLOCKS
+    assert choice[0] in batch.Autotuner.STAGES and choice[1] in batch.Autotuner.HEAVY
     assert tuner.cache[tuner.key(r)] == choice
     assert tuner.tune(r) == choice
-    assert (r.tuning.heavy_window, r.tuning.blocks_per_sm) == choice
+    assert (r.tuning.stage_config, r.tuning.heavy_window) == choice

@@ -14,6 +14,9 @@ atol 5e-3 + rtol 2e-2 (a bf16 emulation of the fp32 oracle differs from the
 reference by at most 9e-4 on the fixture); positions outside the mask are
 exactly zero.
 """
+import ctypes
+import time
+
 import numpy as np
 import pytest
 import torch
@@ -262,3 +265,38 @@ def test_aggregator_after_full_size_sampling():
     want_a, want_c = OD.aggregator(params, *sub[:6], np.ones((1024, 1), bool), sub[6])
     np.testing.assert_allclose(got_a[pick], want_a[:, 0], rtol=AGG_RTOL, atol=AGG_ATOL)
     np.testing.assert_allclose(got_c[pick], want_c[:, 0], rtol=AGG_RTOL, atol=AGG_ATOL)
+
+
+def test_aggregator_wait_gives_up_and_reports():
+    """Failure detection without a fault: the test library's hp_aggregator_forward_withheld never
+    loads one weight block, so the tensor-core warp's bounded wait for it runs out (20 ms here);
+    the kernels return, hp_aggregator_status reports the failure, and the next forward on the same
+    workspace and context is correct again."""
+    native.build_testing()
+    T = native.testing_lib()
+    rng = np.random.default_rng(11)
+    params = {k: ((rng.standard_normal((o, i)) / np.sqrt(i)).astype(np.float32),
+                  (rng.standard_normal(o) * 0.1).astype(np.float32)) for k, o, i in OD.AGG_LAYERS}
+    packed = _agg_pack(params)
+    ins, rays_d, mask = _random_agg_case(rng, 600, 8, 300, 4)
+    ins_d = [D(x) for x in ins]
+    mask_d, rays_d_d = D(mask), D(rays_d)
+    M, P = mask.sum(), 8
+    offsets, _ = ops.mask_scan(mask_d)
+    alphas = torch.empty(mask.shape, dtype=torch.float32, device="cuda")
+    colors = torch.empty(mask.shape + (3,), dtype=torch.float32, device="cuda")
+    ws_bytes = T.hp_aggregator_workspace_size(int(M))
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    t0 = time.perf_counter()
+    rc = T.hp_aggregator_forward_withheld(p(packed), *[p(x) for x in ins_d[:4]], 32, p(ins_d[4]), p(ins_d[5]),
+                                          p(rays_d_d), int(M), P, p(mask_d), p(offsets), mask.size, p(alphas),
+                                          p(colors), p(ws), ws_bytes, 20000, stream)
+    native.check(rc, "hp_aggregator_forward_withheld", T)
+    rc = T.hp_aggregator_status(p(ws), int(M), stream)
+    elapsed = time.perf_counter() - t0
+    assert rc != 0 and "timed out" in T.hp_last_error().decode()
+    assert elapsed < 1.5  # the 20 ms limit ended it, not the default 2 s
+    got = ops.aggregator_forward(packed, *ins_d, mask_d, rays_d_d, check_status=True)
+    _agg_check(got, OD.aggregator(params, *ins, mask, rays_d), mask)

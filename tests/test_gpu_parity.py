@@ -59,6 +59,23 @@ def test_quick_sampling_bit_exact_vs_reference(name):
     assert np.array_equal(bits(H(sp_xyz)), bits(g["sp_xyz"]))
 
 
+@pytest.mark.parametrize("stage", native.STAGE_CONFIGS)
+def test_every_stage_config_bit_exact_vs_reference(stage):
+    """Each stage configuration of the sampling kernel (staged points per tile, blocks per SM)
+    reproduces every golden fixture; the tuning changes speed only."""
+    for name in NAMES:
+        g = Golden(name)
+        for heavy in (0, 1, 4096):  # default, every ray warp-served, none
+            t = ops.make_tuning(heavy_window=heavy, stage_config=stage)
+            sp_xyz, pc_idx, sp_t, mask = ops.quick_sampling(D(g["xyz"]), D(g["c2w"]), g.fx, g.fy, g.cx, g.cy, g.W,
+                                                            g.H, g.opt, D(g["sorted_point_idx"]),
+                                                            D(g["hash_table"]), tuning=t)
+            assert np.array_equal(H(mask), g["mask"]), (name, heavy)
+            assert np.array_equal(H(pc_idx), g["pc_idx"]), (name, heavy)
+            assert np.array_equal(bits(H(sp_t)), bits(g["sp_t"])), (name, heavy)
+            assert np.array_equal(bits(H(sp_xyz)), bits(g["sp_xyz"])), (name, heavy)
+
+
 @pytest.mark.parametrize("name", NAMES)
 def test_scatter_hashtable_bit_exact_vs_reference(name):
     g = Golden(name)
@@ -102,6 +119,34 @@ def test_scatter_multibin_vs_reference(name):
                                           g.H, g.W, bins)
             assert np.array_equal(H(bi), g[k])
             assert np.array_equal(bits(H(bd)), bits(g["scatter_depth_%d" % bins]))
+
+
+# ---------------------------------------------------------------------------
+# projection rounding at the switch points of the reference's cuBLAS GEMMs
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("n", list(range(1, 17)) + [1535, 1536, 1537, 1538, 233022, 233023, 233024, 233025])
+def test_projection_vs_reference_torch(n):
+    """Pixel ids and depths of hp_pts2plane against the reference's own torch projection
+    (epcq.py:251-274, run here with this machine's torch and cuBLAS) at point counts that bracket
+    the GEMM-rounding switch points of hp_projection_rounding.  Depths are compared bit for bit:
+    a wrong rounding form changes most of them by an ulp.  N = 1 (a 3x3 by 3x1 product) matched
+    neither rounding form when the switch points were measured, so there only pixel ids must
+    agree and depths within 1 ulp."""
+    from ref_pipeline import RefPipeline
+    rng = np.random.default_rng(1000 + n)
+    cam = synth.look_at_camera((0.3, -0.2, 4.0), (0, 0, 0), 64, 48, 70.0)
+    xyz = (rng.standard_normal((n, 3)) * 0.5).astype(np.float32)
+    X, w2c, K = D(xyz), D(cam.w2c), D(cam.K)
+    pid, depth, _, _, _ = RefPipeline(None, X.device).project(X, w2c, K, cam.height, cam.width)
+    pid_h, dep_h = H(pid).astype(np.int32), H(depth).astype(np.float32)
+    perm = np.argsort(pid_h, kind="stable").astype(np.int32)
+    r_sidx, r_sdep, r_hsh = O.scatter_hashtable(perm, pid_h[perm], dep_h[perm], cam.height, cam.width, False)
+    sidx, sdep, hsh = (H(t) for t in ops.pts2plane(X, w2c, K, cam.height, cam.width, False))
+    assert np.array_equal(hsh, r_hsh) and np.array_equal(sidx, r_sidx)
+    if n == 1:
+        assert np.all(np.abs(bits(sdep).astype(np.int64) - bits(r_sdep).astype(np.int64)) <= 1)
+    else:
+        assert np.array_equal(bits(sdep), bits(r_sdep))
 
 
 # ---------------------------------------------------------------------------
@@ -222,6 +267,21 @@ def _full(name):
     return sc.xyz, sc.cameras[0], sc.options
 
 
+@pytest.mark.parametrize("name", ["shapes", "clusters"])
+def test_full_size_every_stage_config_identical(name):
+    """At full size every stage configuration gives the default's outputs bit for bit (the
+    configurations split and stage different work items, so they take different code paths)."""
+    xyz, cam, opt = _full(name)
+    X, c2w, w2c, K = D(xyz), D(cam.c2w), D(cam.w2c), D(cam.K)
+    sidx, _, hsh = ops.pts2plane(X, w2c, K, cam.height, cam.width, False)
+    run = lambda t: [H(o) for o in ops.quick_sampling(X, c2w, cam.fx, cam.fy, cam.cx, cam.cy, cam.width, cam.height,
+                                                      opt, sidx, hsh, tuning=t)]
+    base = run(None)
+    for stage in native.STAGE_CONFIGS:
+        for a, b in zip(run(ops.make_tuning(stage_config=stage)), base):
+            assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), stage
+
+
 @pytest.mark.parametrize("name", ["sphere", "shapes", "clusters"])
 def test_full_size(name):
     xyz, cam, opt = _full(name)
@@ -261,6 +321,24 @@ def test_full_size(name):
     assert np.all(d < opt.radius_threshold * (1 + 1e-5))
 
 
+@pytest.mark.parametrize("name", ["sphere", "shapes", "clusters"])
+def test_fp64_error_statement(name):
+    """The FP32 path's error against the FP64 oracle on 4000 sampled rays of a full-size view
+    (oracle/error_stats.py): camera depths and sample depths within 1e-6 relative, sample
+    positions within 1e-5 relative at the 99th percentile, ray distances within 1e-3 of the
+    radius, and rays whose discrete choices differ from FP64 under 1%."""
+    import error_stats
+    xyz, cam, opt = _full(name)
+    (sidx, sdep, hsh), (sp_xyz, pc_idx, sp_t, mask), dirs = _run_case(xyz, cam, opt, False)
+    st = error_stats.fp64_error(xyz, cam, opt, sidx, sdep, hsh, sp_xyz, sp_t, mask, pc_idx, dirs)
+    assert st["depth_rel"]["max"] <= 1e-6, st["depth_rel"]
+    assert st["t_rel"]["n"] > 500 and st["t_rel"]["max"] <= 1e-6, st["t_rel"]
+    assert st["xyz_rel"]["p99"] <= 1e-5, st["xyz_rel"]
+    assert st["ray_dist_abs_over_radius"]["max"] <= 1e-3, st["ray_dist_abs_over_radius"]
+    flips = st["decision_flips"]
+    assert flips["rays_with_other_slots"] + flips["samples_moved"] <= 0.01 * st["rays"], flips
+
+
 # ---------------------------------------------------------------------------
 # the reference's own CUDA build (present when oracle/_ref travels with the repo)
 # ---------------------------------------------------------------------------
@@ -272,15 +350,22 @@ def _ref_module():
     return build_ref.load()
 
 
-@pytest.mark.parametrize("name", ["sphere", "shapes"])
+def _mixed_view_1600():
+    """A 1600x1200 view of the uneven multi-cloud workload (its largest resolution), on its cloud."""
+    mb = synth.make_mixed(n_clouds=8, n_views=64, seed=0)
+    ci, cam = next((c, v) for c, v in mb.views if v.width == 1600)
+    return mb.clouds[ci], cam, mb.options
+
+
+@pytest.mark.parametrize("name", ["sphere", "shapes", "clusters", "mixed_1600x1200"])
 def test_full_size_vs_reference_cuda(name):
-    """Whole pipeline vs the reference's CUDA extension driven as epcq.py drives it (P = 8)."""
-    import sys
-    import os
-    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
-    from make_golden import RefPipeline
+    """Whole pipeline vs the reference's CUDA extension driven as epcq.py drives it (P = 8): the
+    100k-point sphere, the 1M-point shapes view, the 3M-point clusters view at 1600x1200 with
+    K = 16 (deep buckets, the 48-per-cell cap, warp-served and unstaged work), and a 1600x1200
+    view of the uneven multi-cloud workload."""
+    from ref_pipeline import RefPipeline
     mod = _ref_module()
-    xyz, cam, opt = _full(name)
+    xyz, cam, opt = _mixed_view_1600() if name == "mixed_1600x1200" else _full(name)
     rp = RefPipeline(mod, torch.device("cuda:0"))
     X = D(xyz)
     c2w, w2c, K = D(cam.c2w), D(cam.w2c), D(cam.K)

@@ -25,7 +25,7 @@ PLAIN, SW128, SW64 = 0, 1, 2
 
 @pytest.fixture(scope="module", autouse=True)
 def _setup():
-    native.build()
+    native.build_testing()
 
 
 def plain_offset(r, k):
@@ -72,7 +72,7 @@ def window_start(form, k0, rows):
 
 def run_case(a_form, a_k, a_k0, b_form, b_k, b_k0, live, seed):
     """One MMA over A's K columns a_k0.. and B's b_k0..; only the first `live` of the 16 are nonzero."""
-    L = native.lib()
+    L = native.testing_lib()
     rng = np.random.default_rng(seed)
     A = rng.integers(-3, 4, (128, a_k)).astype(np.float32)
     B = rng.integers(-3, 4, (256, b_k)).astype(np.float32)
@@ -83,7 +83,7 @@ def run_case(a_form, a_k, a_k0, b_form, b_k, b_k0, live, seed):
     d = torch.empty(128, 256, dtype=torch.float32, device="cuda")
     rc = L.hp_tc_check_mma(a_img.data_ptr(), b_img.data_ptr(), a_form, window_start(a_form, a_k0, 128), b_form,
                            window_start(b_form, b_k0, 256), d.data_ptr(), torch.cuda.current_stream().cuda_stream)
-    native.check(rc, "hp_tc_check_mma")
+    native.check(rc, "hp_tc_check_mma", L)
     want = A[:, a_k0:a_k0 + 16] @ B[:, b_k0:b_k0 + 16].T
     return d.cpu().numpy(), want
 
@@ -115,7 +115,7 @@ def test_operand_forms(case):
 
 
 def test_rejects_windows_outside_the_image():
-    L = native.lib()
+    L = native.testing_lib()
     a = torch.zeros(L.hp_tc_check_image_bytes(0), dtype=torch.uint8, device="cuda")
     b = torch.zeros(L.hp_tc_check_image_bytes(1), dtype=torch.uint8, device="cuda")
     d = torch.empty(128, 256, dtype=torch.float32, device="cuda")

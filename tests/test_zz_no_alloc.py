@@ -16,6 +16,7 @@ import numpy as np
 import pytest
 import torch
 
+import oracle as O
 from hashpoint import native, ops, synth
 
 pytestmark = pytest.mark.gpu
@@ -59,6 +60,33 @@ def test_noalloc_matches_workspace_entry_point_on_two_calls():
         assert torch.equal(a[2], b[2])
         assert torch.equal(a[1].view(torch.int32), b[1].view(torch.int32))
         assert int((a[2][:, 1] > 0).sum()) > 0
+
+
+def test_noalloc_at_its_limits():
+    """Exactly the largest problem the built-in scratch takes (262144 points on a 1024 x 1024
+    image, whose scratch offsets are the tightest), checked against hp_pts2plane and the CPU
+    oracle; then no points at all on the same image."""
+    native.build()
+    O.build()
+    rng = np.random.default_rng(13)
+    xyz = synth.shapes_cloud(rng, MAX_POINTS)
+    cam = synth.orbit_cameras(rng, 1, 4.0, 1024, 1024, 1400.0)[0]
+    assert cam.width * cam.height == MAX_PIXELS
+    dev = torch.device("cuda:0")
+    X, w2c, K = (torch.from_numpy(a).to(dev) for a in (xyz, cam.w2c, cam.K))
+    for sort in (False, True):
+        a = _noalloc(X, w2c, K, cam.height, cam.width, sort)
+        b = ops.pts2plane(X, w2c, K, cam.height, cam.width, sort)
+        torch.cuda.synchronize()
+        for x, y in zip(a, b):
+            assert torch.equal(x.view(torch.int32), y.view(torch.int32))
+        oi, od, oh = O.pts2plane(xyz, O.camera_from(cam), sort)
+        assert np.array_equal(a[0].cpu().numpy(), oi) and np.array_equal(a[2].cpu().numpy(), oh)
+        assert np.array_equal(a[1].cpu().numpy().view(np.int32), od.view(np.int32))
+    empty = torch.empty((0, 3), dtype=torch.float32, device=dev)
+    sidx, sdep, hsh = _noalloc(empty, w2c, K, cam.height, cam.width, False)
+    torch.cuda.synchronize()
+    assert sidx.numel() == 0 and sdep.numel() == 0 and bool((hsh == -1).all())
 
 
 def test_noalloc_refuses_problems_beyond_its_scratch():
