@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-systems", action="store_true", help="skip the batched and served measurements")
     ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--served-only", action="store_true",
+                    help="run only the served measurement and print its JSON (the main run starts this in a fresh "
+                         "process)")
     ap.add_argument("--kernels-once", action="store_true",
                     help="run one view of the workload once through every kernel of the path and exit (for profilers)")
     ap.add_argument("--agg-case", type=int, default=0, metavar="N",
@@ -125,6 +128,15 @@ def cpu_baseline(n_views=3, scene=None, searchers=True, error_views=None):
         import error_stats
         out["fp64_error"] = {name: error_stats.fp64_error(*v, nthreads=cores) for name, v in error_views.items()}
     return out
+
+
+def stage_desc(stage_config, heavy_window=None):
+    """A tuning choice as the tile, stage capacity and occupancy it stands for."""
+    from hashpoint import native
+    d = {"stage_config": int(stage_config), **native.stage_config_info(stage_config)}
+    if heavy_window is not None:
+        d["heavy_window"] = int(heavy_window)
+    return d
 
 
 # ---------------------------------------------------------------------------
@@ -214,6 +226,10 @@ def run_gpu(args):
     structs = [cams.struct(i) for i in range(cams.n)]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
+    # the sampling kernel's stage configuration for this workload (outputs never depend on it)
+    with torch.cuda.stream(stream):
+        stage = pipe.tune(xyz, structs[:5], stream)
+
     # in-image point count per view (for the algorithmic byte count), outside timing
     n_in = []
     with torch.cuda.stream(stream):
@@ -293,7 +309,7 @@ def run_gpu(args):
     # workloads, and the reference's own CUDA path on the same GPU
     batched = served = downstream = others = refgpu = error_views = None
     if world == 1 and not args.no_systems:
-        served = run_served(args, dev)  # first: the real-time loop is the most sensitive to the process's state
+        served = run_served_isolated(args)  # a process of its own: the real-time loop is sensitive to process state
         torch.cuda.empty_cache()
         downstream = run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
         others = run_other_workloads(dev, flush, peak)
@@ -314,7 +330,7 @@ def run_gpu(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no public dataset)",
         "config": config_dict(args, {"l2": "flushed between steps (256 MiB write)",
                                      "path": "plain per-view launch, preallocated buffers",
-                                     "sampling_stage_config": "default (hp_tuning.stage_config 0)"}),
+                                     "sampling_stage_config": stage_desc(stage)}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "k_quick_sampling", "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": sum(samp_bytes) / len(samp_bytes),
@@ -517,8 +533,9 @@ def sampling_bytes(n_in, H, W, S, P):
 
 def run_other_workloads(dev, flush, peak):
     """The 100k-point sphere at 400x400 (k=3) and the 3M-point clusters at 1600x1200 (K=16) through
-    the same plain per-view launch (CUDA events, L2 flushed before each view): build + sample per
-    view, the sampling launch alone, and its fraction of the HBM roofline."""
+    the same plain per-view launch (CUDA events, L2 flushed before each view), with the stage
+    configuration the pipeline's tune() picks for the workload: build + sample per view, the
+    sampling launch alone, and its fraction of the HBM roofline."""
     import torch
 
     from hashpoint import synth
@@ -532,6 +549,7 @@ def run_other_workloads(dev, flush, peak):
         cams = CameraTable(sc.cameras, dev)
         structs = [cams.struct(i) for i in range(cams.n)]
         st = torch.cuda.current_stream(dev)
+        stage = pipe.tune(X, structs[:2], st)
         n_in = []
         for s_ in structs:
             pipe.render(X, s_)
@@ -554,7 +572,7 @@ def run_other_workloads(dev, flush, peak):
         nbytes = sum(sampling_bytes(ni, c0.height, c0.width, S, P) for ni in n_in) / len(n_in)
         achieved = nbytes / (sms * 1e-3) / 1e9
         out[name] = {"rays_per_s": c0.width * c0.height / (ms * 1e-3), "ms_per_view": ms, "sample_ms": sms,
-                     "views": len(structs), "points": len(sc.xyz),
+                     "views": len(structs), "points": len(sc.xyz), "sampling_stage_config": stage_desc(stage),
                      "roofline": {"bound": "hbm", "kernel": "k_quick_sampling", "achieved": achieved, "peak": peak,
                                   "unit": "GB/s", "frac": achieved / peak, "algorithmic_bytes_per_launch": nbytes}}
         del pipe, X
@@ -654,7 +672,7 @@ def run_batched(args, dev, xyz, sc, flush):
     pv = _event_ms(r.run_per_view, 3, flush)
     g = _event_ms(r.replay, max(args.steps, 3), flush)
     out["shapes_100views"] = {"rays_per_s": r.rays / (g * 1e-3), "ms": g, "per_view_rays_s": r.rays / (pv * 1e-3),
-                              "per_view_ms": pv, "speedup": pv / g, "tuning": list(tuning),
+                              "per_view_ms": pv, "speedup": pv / g, "tuning": stage_desc(*tuning),
                               "path": "hp_pts2plane x100 on 4 streams + one hp_quick_sampling_batch, CUDA graph"}
     r.release()
     del r
@@ -672,10 +690,27 @@ def run_batched(args, dev, xyz, sc, flush):
     g = _event_ms(r.replay, max(args.steps, 3), flush)
     out["mixed_64views_8clouds"] = {
         "rays_per_s": r.rays / (g * 1e-3), "ms": g, "per_view_rays_s": r.rays / (pv * 1e-3), "per_view_ms": pv,
-        "speedup": pv / g, "tuning": list(tuning), "rays": r.rays, "points": [int(c.shape[0]) for c in clouds],
+        "speedup": pv / g, "tuning": stage_desc(*tuning), "rays": r.rays, "points": [int(c.shape[0]) for c in clouds],
         "path": "one CUDA graph: 64 hash-table builds on 4 streams + one persistent sampling launch"}
     r.release()
     del r, clouds
+    return out
+
+
+def run_served_isolated(args):
+    """run_served in a fresh process on the same GPU, as a server would run: the request loop is
+    a real-time host loop, and in the benchmark process -- after the timed sections' allocations,
+    streams and host threads -- its latency was an order of magnitude worse than in a process of
+    its own on the same machine."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--served-only", "--serve-requests", str(args.serve_requests)]
+    env = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    p = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, env=env, timeout=1200)
+    if p.returncode != 0:
+        return {"unavailable": "served run failed: " + p.stderr.strip().splitlines()[-1][:200] if p.stderr else "?"}
+    out = json.loads(p.stdout.strip().splitlines()[-1])
+    out["process"] = "fresh (bench.py --served-only)"
     return out
 
 
@@ -702,12 +737,18 @@ def run_served(args, dev):
     serve.Server(store, budget).run(requests(2000.0, n))  # warm: hash-table cache and allocator
 
     def median_run(rate, count, runs=3):
-        # batch formation under a Poisson arrival stream depends on timing, so single runs vary by
-        # +-20%: report the run with the median rays/s and the spread
-        res = sorted((serve.Server(store, budget).run(requests(rate, count)) for _ in range(runs)),
-                     key=lambda r: r["rays_per_s"] or 0)
+        # The first run meets cold hash-table caches (every new scene/pose builds its table);
+        # it is reported on its own as the cold start.  Batch formation under a Poisson arrival
+        # stream depends on timing, so warm runs vary too: report the warm run with the median
+        # p50 and every run's figures in order.
+        cold = serve.Server(store, budget).run(requests(rate, count))
+        runs_ = [serve.Server(store, budget).run(requests(rate, count)) for _ in range(runs)]
+        res = sorted(runs_, key=lambda r: r["p50_ms"])
         med = dict(res[len(res) // 2])
-        med["runs_rays_per_s"] = [r["rays_per_s"] for r in res]
+        med["runs_rays_per_s"] = [r["rays_per_s"] for r in runs_]
+        keys = ("p50_ms", "p99_ms", "batches", "cache_misses")
+        med["cold_run"] = {k: cold[k] for k in keys}
+        med["runs_in_order"] = [{k: r[k] for k in keys} for r in runs_]
         return med
 
     hot = median_run(2000.0, n)
@@ -728,13 +769,16 @@ def run_served(args, dev):
     ser = _event_ms(serial, 1)
     rays = sum(q.rays for q in reqs)
     keep = ("requests", "done", "rejected", "batches", "p50_ms", "p99_ms", "mean_ms", "rays_per_s", "span_ms",
-            "runs_rays_per_s")
+            "runs_rays_per_s", "cache_hits", "cache_misses", "cold_run", "runs_in_order")
     return {"scenes": len(clouds), "points": int(sum(len(c) for c in clouds)), "budget_gb": 120,
             "lambda_2000": {k: hot[k] for k in keep}, "lambda_200": {k: light[k] for k in keep},
             "serial_plain_rays_per_s": rays / (ser * 1e-3), "serial_plain_ms": ser,
             "speedup_vs_serial_plain": (hot["rays_per_s"] or 0) / (rays / (ser * 1e-3)),
-            "note": "median of 3 runs each; at 2000 requests/s the offered load exceeds the GPU's capacity, "
-                    "so latency is mostly queueing; 200 requests/s is below it"}
+            "note": "one cold run (cold_run: every scene/pose table built on first use), then the warm run "
+                    "with the median p50 of 3; at 2000 requests/s the offered load exceeds the GPU's capacity, "
+                    "so latency is mostly queueing; 200 requests/s is below it; cameras: 16 fixed poses per scene "
+                    "(hash tables cached per scene, pose and resolution); cache_misses counts the tables built "
+                    "during the reported run"}
 
 
 def run_reference(args):
@@ -841,7 +885,12 @@ def run_agg_case(n):
 
 def main():
     args = parse()
-    if args.kernels_once:
+    if args.served_only:
+        import torch
+        from hashpoint import native
+        native.build()
+        print(json.dumps(run_served(args, torch.device("cuda", 0))), flush=True)
+    elif args.kernels_once:
         run_kernels_once(args)
     elif args.agg_case > 0:
         run_agg_case(args.agg_case)

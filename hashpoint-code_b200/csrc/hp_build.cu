@@ -10,12 +10,15 @@
 //                     exact rounding, atomic slot within the pixel's bucket
 //   k_block_sums      per-block totals of the H*W counts
 //   k_scan_hash       exclusive scan -> hash_table (start, count) / (-1, -1)
-//   k_scatter         every point to start + slot of a scratch copy (id, depth,
-//                     pixel); -1 into the off-image tail of the outputs
+//   k_scatter         every point to start + slot of a scratch copy, one
+//                     16-byte (id, depth, pixel) record per entry; -1 into the
+//                     off-image tail of the outputs
 //   k_order           one thread per bucket entry: its rank among its bucket's
 //                     entries gives its final position (buckets <= 2048)
-//   k_sort_huge       buckets above 2048 entries: one CTA each, bitonic sort
-//                     in place in global memory
+//   k_sort_huge_list  buckets above 2048 entries, which k_scan_hash lists as
+//                     it writes the table: one CTA each, bitonic sort in place
+//                     in global memory (k_sort_huge_scan finds them by
+//                     scanning the table where there is no workspace)
 //
 // The atomic slots make the order inside a bucket arbitrary; ranking restores
 // the reference's order: ascending point id (the stable sort's order) when
@@ -117,9 +120,12 @@ __global__ void __launch_bounds__(kScanThreads) k_block_sums(const int* __restri
 
 // Exclusive scan of counts -> hash_table; the block's carry-in is the sum of
 // the preceding blocks' totals.
+// Also lists the pixels whose buckets exceed kRankMax (count in scalars[1]),
+// for k_sort_huge_list.
 __global__ void __launch_bounds__(kScanThreads) k_scan_hash(const int* __restrict__ counts, int hw,
                                                             const int* __restrict__ block_sums,
-                                                            int2* __restrict__ hash, int* __restrict__ scalars) {
+                                                            int2* __restrict__ hash, int* __restrict__ scalars,
+                                                            int* __restrict__ huge) {
   __shared__ int sh[32];
   __shared__ int warp_tot[32];
   int carry = 0;
@@ -161,6 +167,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_hash(const int* __restric
     const int p = base + j;
     if (p < hw) {
       hash[p] = c[j] > 0 ? make_int2(off, c[j]) : make_int2(-1, -1);
+      if (c[j] > kRankMax) huge[atomicAdd(scalars + 1, 1)] = p;
     }
     off += c[j];
   }
@@ -172,18 +179,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_hash(const int* __restric
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_scatter(int n, int hw, const int2* __restrict__ pid_slot,
                                                  const float* __restrict__ depth, const int2* __restrict__ hash,
-                                                 const int* __restrict__ scalars, int* __restrict__ tmp_id,
-                                                 float* __restrict__ tmp_depth, int* __restrict__ tmp_pid,
+                                                 const int* __restrict__ scalars, int4* __restrict__ tmp,
                                                  int* __restrict__ out_idx, float* __restrict__ out_depth) {
   const int n_in = scalars[0];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int2 ps = pid_slot[i];
-    if (ps.x < hw) {
-      const int pos = hash[ps.x].x + ps.y;
-      tmp_id[pos] = i;
-      tmp_depth[pos] = depth[i];
-      tmp_pid[pos] = ps.x;
-    }
+    if (ps.x < hw) tmp[hash[ps.x].x + ps.y] = make_int4(i, __float_as_int(depth[i]), ps.x, 0);
     if (i >= n_in) {
       out_idx[i] = -1;
       out_depth[i] = -1.0f;
@@ -206,30 +207,51 @@ __device__ __forceinline__ unsigned long long entry_key(const BucketOrder& bo, i
   return sort_key(bo.by_position ? pos : id, depth, bo.by_depth);
 }
 
+// Bucket entries in position order: hp_pts2plane's packed scratch records ...
+struct PackedEntries {
+  const int4* rec;  // (id, depth bits, pixel, 0)
+  __device__ __forceinline__ int pixel(int j) const { return __ldg(&rec[j].z); }
+  __device__ __forceinline__ int2 id_depth(int j) const { return __ldg(reinterpret_cast<const int2*>(rec + j)); }
+};
+
+// ... or the caller's sorted arrays (hp_scatter_hashtable).
+struct SplitEntries {
+  const int* id;
+  const float* depth;
+  const int* pid;
+  __device__ __forceinline__ int pixel(int j) const { return __ldg(pid + j); }
+  __device__ __forceinline__ int2 id_depth(int j) const {
+    return make_int2(__ldg(id + j), __float_as_int(__ldg(depth + j)));
+  }
+};
+
 // One thread per entry j < n_in of the scratch copy: rank among the entries of
 // its bucket -> final position.  Buckets of one entry are copied; buckets above
-// kRankMax are left to k_sort_huge.
-__global__ void __launch_bounds__(256) k_order(const int* __restrict__ in_id, const float* __restrict__ in_depth,
-                                               const int* __restrict__ in_pid, const int2* __restrict__ hash, int hw,
+// kRankMax are left to k_sort_huge_list / k_sort_huge_scan.
+template <class Entries>
+__global__ void __launch_bounds__(256) k_order(Entries in, const int2* __restrict__ hash, int hw,
                                                const int* __restrict__ scalars, int n_fixed,
                                                int* __restrict__ out_idx, float* __restrict__ out_depth,
                                                BucketOrder bo) {
   const int n_in = n_fixed >= 0 ? n_fixed : scalars[0];
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_in; j += gridDim.x * blockDim.x) {
-    const int p = in_pid[j];
+    const int p = in.pixel(j);
     if (p < 0 || p >= hw) continue;
     const int2 h = hash[p];
-    const int id = in_id[j];
-    const float d = in_depth[j];
     if (h.y > kRankMax) continue;
+    const int2 e = in.id_depth(j);
+    const float d = __int_as_float(e.y);
     int pos = h.x;
     if (h.y > 1) {
-      const unsigned long long kj = entry_key(bo, id, d, j);
+      const unsigned long long kj = entry_key(bo, e.x, d, j);
       int rank = 0;
-      for (int q = h.x; q < h.x + h.y; q++) rank += entry_key(bo, __ldg(in_id + q), __ldg(in_depth + q), q) < kj;
+      for (int q = h.x; q < h.x + h.y; q++) {
+        const int2 eq = in.id_depth(q);
+        rank += entry_key(bo, eq.x, __int_as_float(eq.y), q) < kj;
+      }
       pos += rank;
     }
-    out_idx[pos] = id;
+    out_idx[pos] = e.x;
     out_depth[pos] = d;
   }
 }
@@ -251,15 +273,61 @@ __device__ __forceinline__ void cx_global(const BucketOrder& bo, int* idx, float
   }
 }
 
-// Buckets above kRankMax entries (pathological inputs): each CTA scans a
-// contiguous range of pixels blockDim at a time, queues the huge ones in shared
-// memory, and sorts each in place in global memory after copying it from the
-// scratch arrays (in_id / in_depth, indexed by position).
-__global__ void __launch_bounds__(kHugeThreads) k_sort_huge(int hw, const int* __restrict__ in_id,
-                                                            const float* __restrict__ in_depth,
-                                                            const int2* __restrict__ hash,
-                                                            int* __restrict__ out_idx, float* __restrict__ out_depth,
-                                                            BucketOrder bo) {
+// One bucket above kRankMax entries (pathological inputs), sorted by one CTA in
+// place in global memory after copying it from the scratch entries (indexed by
+// position).
+template <class Entries>
+__device__ __forceinline__ void sort_bucket(int2 h, Entries in, int* __restrict__ out_idx, float* __restrict__ out_depth,
+                                            const BucketOrder& bo) {
+  const int c = h.y;
+  int* idx = out_idx + h.x;
+  float* dep = out_depth + h.x;
+  for (int i = threadIdx.x; i < c; i += blockDim.x) {
+    const int2 e = in.id_depth(h.x + i);
+    idx[i] = bo.by_position ? h.x + i : e.x;
+    dep[i] = __int_as_float(e.y);
+  }
+  __syncthreads();
+  int npow = 1;
+  while (npow < c) npow <<= 1;
+  for (int k = 2; k <= npow; k <<= 1) {
+    for (int i = threadIdx.x; i < npow / 2; i += blockDim.x) {
+      const int blk = i / (k >> 1), off = i % (k >> 1);
+      const int a = blk * k + off, b = blk * k + k - 1 - off;
+      if (a < c) cx_global(bo, idx, dep, a, b, c);
+    }
+    __syncthreads();
+    for (int j = k >> 2; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < npow / 2; i += blockDim.x) {
+        const int blk = i / j, off = i % j;
+        const int a = blk * 2 * j + off;
+        if (a < c) cx_global(bo, idx, dep, a, a + j, c);
+      }
+      __syncthreads();
+    }
+  }
+  if (bo.by_position)
+    for (int i = threadIdx.x; i < c; i += blockDim.x) idx[i] = in.id_depth(idx[i]).x;
+  __syncthreads();
+}
+
+// hp_pts2plane: the buckets k_scan_hash listed, one CTA each in turn.
+template <class Entries>
+__global__ void __launch_bounds__(kHugeThreads) k_sort_huge_list(const int* __restrict__ huge,
+                                                                 const int* __restrict__ scalars, Entries in,
+                                                                 const int2* __restrict__ hash,
+                                                                 int* __restrict__ out_idx,
+                                                                 float* __restrict__ out_depth, BucketOrder bo) {
+  const int n = scalars[1];
+  for (int q = blockIdx.x; q < n; q += gridDim.x) sort_bucket(hash[huge[q]], in, out_idx, out_depth, bo);
+}
+
+// hp_scatter_hashtable (no workspace for a list): each CTA scans a contiguous
+// range of pixels blockDim at a time and queues the huge ones in shared memory.
+template <class Entries>
+__global__ void __launch_bounds__(kHugeThreads) k_sort_huge_scan(int hw, Entries in, const int2* __restrict__ hash,
+                                                                 int* __restrict__ out_idx,
+                                                                 float* __restrict__ out_depth, BucketOrder bo) {
   __shared__ int queue[kHugeThreads];
   __shared__ int qn;
   const int per = (hw + gridDim.x - 1) / gridDim.x;
@@ -271,38 +339,7 @@ __global__ void __launch_bounds__(kHugeThreads) k_sort_huge(int hw, const int* _
     if (p < hi && hash[p].y > kRankMax) queue[atomicAdd(&qn, 1)] = p;
     __syncthreads();
     const int nq = qn;
-    for (int q = 0; q < nq; q++) {
-      const int2 h = hash[queue[q]];
-      const int c = h.y;
-      int* idx = out_idx + h.x;
-      float* dep = out_depth + h.x;
-      for (int i = threadIdx.x; i < c; i += blockDim.x) {
-        idx[i] = bo.by_position ? h.x + i : in_id[h.x + i];
-        dep[i] = in_depth[h.x + i];
-      }
-      __syncthreads();
-      int npow = 1;
-      while (npow < c) npow <<= 1;
-      for (int k = 2; k <= npow; k <<= 1) {
-        for (int i = threadIdx.x; i < npow / 2; i += blockDim.x) {
-          const int blk = i / (k >> 1), off = i % (k >> 1);
-          const int a = blk * k + off, b = blk * k + k - 1 - off;
-          if (a < c) cx_global(bo, idx, dep, a, b, c);
-        }
-        __syncthreads();
-        for (int j = k >> 2; j > 0; j >>= 1) {
-          for (int i = threadIdx.x; i < npow / 2; i += blockDim.x) {
-            const int blk = i / j, off = i % j;
-            const int a = blk * 2 * j + off;
-            if (a < c) cx_global(bo, idx, dep, a, a + j, c);
-          }
-          __syncthreads();
-        }
-      }
-      if (bo.by_position)
-        for (int i = threadIdx.x; i < c; i += blockDim.x) idx[i] = in_id[idx[i]];
-      __syncthreads();
-    }
+    for (int q = 0; q < nq; q++) sort_bucket(hash[queue[q]], in, out_idx, out_depth, bo);
     __syncthreads();
   }
 }
@@ -337,7 +374,7 @@ __global__ void __launch_bounds__(256) k_runs(const int* __restrict__ point_idx,
 static constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct BuildLayout {
-  size_t counts, block_sums, pid_slot, depth, tmp_id, tmp_depth, tmp_pid, scalars, total;
+  size_t counts, block_sums, pid_slot, depth, tmp, huge, scalars, total;
 };
 
 static BuildLayout build_layout(int64_t n, int64_t hw) {
@@ -352,12 +389,10 @@ static BuildLayout build_layout(int64_t n, int64_t hw) {
   o += align256(sizeof(int2) * (size_t)(n > 0 ? n : 1));
   L.depth = o;
   o += align256(sizeof(float) * (size_t)(n > 0 ? n : 1));
-  L.tmp_id = o;
-  o += align256(sizeof(int) * (size_t)(n > 0 ? n : 1));
-  L.tmp_depth = o;
-  o += align256(sizeof(float) * (size_t)(n > 0 ? n : 1));
-  L.tmp_pid = o;
-  o += align256(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  L.tmp = o;
+  o += align256(sizeof(int4) * (size_t)(n > 0 ? n : 1));
+  L.huge = o;  // pixels of buckets above kRankMax entries: at most n / (kRankMax + 1)
+  o += align256(sizeof(int) * (size_t)(n / (kRankMax + 1) + 1));
   L.scalars = o;
   o += 256;
   L.total = o;
@@ -371,19 +406,24 @@ static int grid_for(int64_t n, int threads) {
   return (int)(g > 0 ? g : 1);
 }
 
-// Bucket order shared by hp_pts2plane (entries in scratch arrays, count on
-// the device) and hp_scatter_hashtable (entries in the caller's sorted input).
-static int32_t launch_order(int hw, int n_fixed, int n_grid, const int* in_id, const float* in_depth, const int* in_pid,
-                            const int2* hash, const int* scalars, int* out_idx, float* out_depth, BucketOrder bo,
-                            cudaStream_t st) {
+// Bucket order shared by hp_pts2plane (packed scratch records, count on the
+// device) and hp_scatter_hashtable (entries in the caller's sorted input).
+// huge: the list of buckets above kRankMax (count in scalars[1]), or null to
+// find them by scanning the hash table.
+template <class Entries>
+static int32_t launch_order(int hw, int n_fixed, int n_grid, Entries in, const int2* hash, const int* scalars,
+                            const int* huge, int* out_idx, float* out_depth, BucketOrder bo, cudaStream_t st) {
   if (n_grid > 0) {
-    k_order<<<grid_for(n_grid, 256), 256, 0, st>>>(in_id, in_depth, in_pid, hash, hw, scalars, n_fixed, out_idx,
-                                                    out_depth, bo);
+    k_order<<<grid_for(n_grid, 256), 256, 0, st>>>(in, hash, hw, scalars, n_fixed, out_idx, out_depth, bo);
     if (int32_t rc = check_launch("k_order")) return rc;
   }
+  if (huge) {
+    k_sort_huge_list<<<148, kHugeThreads, 0, st>>>(huge, scalars, in, hash, out_idx, out_depth, bo);
+    return check_launch("k_sort_huge_list");
+  }
   const int blocks = (hw + kHugeThreads - 1) / kHugeThreads < 148 * 2 ? (hw + kHugeThreads - 1) / kHugeThreads : 148 * 2;
-  k_sort_huge<<<blocks, kHugeThreads, 0, st>>>(hw, in_id, in_depth, hash, out_idx, out_depth, bo);
-  return check_launch("k_sort_huge");
+  k_sort_huge_scan<<<blocks, kHugeThreads, 0, st>>>(hw, in, hash, out_idx, out_depth, bo);
+  return check_launch("k_sort_huge_scan");
 }
 
 }  // namespace hp
@@ -428,9 +468,8 @@ extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_cam
   int* block_sums = (int*)(ws + L.block_sums);
   int2* pid_slot = (int2*)(ws + L.pid_slot);
   float* depth = (float*)(ws + L.depth);
-  int* tmp_id = (int*)(ws + L.tmp_id);
-  float* tmp_depth = (float*)(ws + L.tmp_depth);
-  int* tmp_pid = (int*)(ws + L.tmp_pid);
+  int4* tmp = (int4*)(ws + L.tmp);
+  int* huge = (int*)(ws + L.huge);
   int* scalars = (int*)(ws + L.scalars);
   int2* hash = (int2*)hash_table;
   const int n = (int)n_points;
@@ -448,14 +487,14 @@ extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_cam
   const int nblk = (int)((hw + kScanTile - 1) / kScanTile);
   k_block_sums<<<nblk, kScanThreads, 0, st>>>(counts, (int)hw, block_sums);
   if (int32_t rc = check_launch("k_block_sums")) return rc;
-  k_scan_hash<<<nblk, kScanThreads, 0, st>>>(counts, (int)hw, block_sums, hash, scalars);
+  k_scan_hash<<<nblk, kScanThreads, 0, st>>>(counts, (int)hw, block_sums, hash, scalars, huge);
   if (int32_t rc = check_launch("k_scan_hash")) return rc;
   if (n > 0) {
-    k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, (int)hw, pid_slot, depth, hash, scalars, tmp_id, tmp_depth, tmp_pid,
-                                                sorted_point_idx, sorted_depth);
+    k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, (int)hw, pid_slot, depth, hash, scalars, tmp, sorted_point_idx,
+                                                sorted_depth);
     if (int32_t rc = check_launch("k_scatter")) return rc;
   }
-  return launch_order((int)hw, -1, n, tmp_id, tmp_depth, tmp_pid, hash, scalars, sorted_point_idx, sorted_depth,
+  return launch_order((int)hw, -1, n, PackedEntries{tmp}, hash, scalars, huge, sorted_point_idx, sorted_depth,
                       BucketOrder{sort != 0, 0}, st);
 }
 
@@ -483,8 +522,8 @@ extern "C" int32_t hp_scatter_hashtable(const int32_t* point_idx, const int32_t*
   }
   if (!sort) return HP_OK;
   // depth order inside each run, ties kept in input order
-  return launch_order(hw, (int)n, (int)n, point_idx, depth, point2img, hash, nullptr, sorted_point_idx, sorted_depth,
-                      BucketOrder{1, 1}, st);
+  return launch_order(hw, (int)n, (int)n, SplitEntries{point_idx, depth, point2img}, hash, nullptr, nullptr,
+                      sorted_point_idx, sorted_depth, BucketOrder{1, 1}, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -500,7 +539,8 @@ constexpr int64_t kNoAllocMaxPixels = HP_NOALLOC_MAX_PIXELS;
 constexpr size_t kNoAllocScratchBytes =
     align256(sizeof(int) * kNoAllocMaxPixels) +
     align256(sizeof(int) * ((kNoAllocMaxPixels + kScanTile - 1) / kScanTile)) +
-    align256(sizeof(int2) * kNoAllocMaxPoints) + 4 * align256(sizeof(float) * kNoAllocMaxPoints) + 256;
+    align256(sizeof(int2) * kNoAllocMaxPoints) + align256(sizeof(float) * kNoAllocMaxPoints) +
+    align256(sizeof(int4) * kNoAllocMaxPoints) + align256(sizeof(int) * (kNoAllocMaxPoints / (kRankMax + 1) + 1)) + 256;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 // Device address of g_noalloc_scratch per device.  It is looked up again on

@@ -51,12 +51,7 @@
 
 namespace hp {
 
-constexpr int kTileW = 32;   // pixels of one image row per warp
-constexpr int kTileH = 8;    // rows per block
-constexpr int kThreads = kTileW * kTileH;
-constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
-constexpr int kCellsPerThread = (kHaloMax + kThreads - 1) / kThreads;
-constexpr int kItemsPerTile = kTileH * 4;  // rows, each in up to four column quarters
+constexpr int kThreads = 256;  // threads of a sampling block = pixels of a tile
 #ifndef HP_BIN_LIST
 #define HP_BIN_LIST 6
 #endif
@@ -86,30 +81,42 @@ struct SampleArgs {
 };
 
 // Stage configurations: kCap staged points per tile, kBlocks resident blocks
-// per SM.  Shared memory per SM bounds the two together (and registers per
+// per SM, and the tile: kTileH rows x kTileW pixels (kThreads in all).
+// Shared memory per SM bounds stage and blocks together (and registers per
 // thread follow from the blocks: 64 at 4 blocks, 80 at 3, 128 at 2).  A larger
 // stage splits fewer dense tiles into row bands (less re-staging of shared
-// halo rows) but keeps fewer warps resident; which wins depends on how the
-// cloud's points spread over the image, so the launch picks one
-// (hp_tuning.stage_config) and hashpoint.batch.Autotuner searches them.
-template <int kCap_, int kBlocks_>
+// halo rows) but keeps fewer warps resident; a square tile stages a smaller
+// window halo per ray (20 x 20 cells for 256 rays against 12 x 36 at k = 5).
+// Which wins depends on how the cloud's points spread over the image, so the
+// launch picks one (hp_tuning.stage_config) and hashpoint.batch.Autotuner
+// searches them.
+template <int kCap_, int kBlocks_, int kTileH_, int kTileW_>
 struct StageCfg {
   static constexpr int kCap = kCap_;
   static constexpr int kBlocks = kBlocks_;
+  static constexpr int kTileH = kTileH_;
+  static constexpr int kTileW = kTileW_;
+  static constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
+  static constexpr int kItemsPerTile = kTileH * 4;  // rows, each in up to four column quarters
+  static_assert(kTileH * kTileW == kThreads && kTileW >= 4 && kTileW <= 32 && kTileH <= 16, "tile shape");
 };
-using Cfg2560x4 = StageCfg<2560, 4>;  // 40 KB stage, 4 blocks per SM (the default)
-using Cfg3712x3 = StageCfg<3712, 3>;  // 58 KB stage, 3 blocks per SM
-using Cfg5888x2 = StageCfg<5888, 2>;  // 92 KB stage, 2 blocks per SM
-constexpr int kStageConfigs = 3;      // hp_tuning.stage_config 1..3 (0 = the default, 1)
+using Cfg2560x4 = StageCfg<2560, 4, 8, 32>;     // 40 KB stage, 4 blocks per SM, 8 x 32 tiles (the default)
+using Cfg3712x3 = StageCfg<3712, 3, 8, 32>;     // 58 KB stage, 3 blocks per SM
+using Cfg5888x2 = StageCfg<5888, 2, 8, 32>;     // 92 KB stage, 2 blocks per SM
+using Cfg2560x4Sq = StageCfg<2560, 4, 16, 16>;  // 16 x 16 tiles
+using Cfg3712x3Sq = StageCfg<3712, 3, 16, 16>;
+constexpr int kStageConfigs = 5;      // hp_tuning.stage_config 1..5 (0 = the default, 1)
+constexpr int kMaxItemsPerTile = 64;  // over the configurations (16 rows, four column ranges each)
+constexpr int kCellsPerThread = 2;    // halo cells per thread (<= 432 = the largest halo)
 
-template <int kCap>
+template <class Cfg>
 struct Stage {
-  float4 cand[kCap];        // x, y, z, id (as int bits; -1 = invalid id)
+  float4 cand[Cfg::kCap];   // x, y, z, id (as int bits; -1 = invalid id)
   int cls[kClasses];        // rays per window-size class
   int cls_base[kClasses];   // first rank of each class
   int order[kThreads];      // pixel of each rank, heaviest class first
-  int off[kHaloMax + 1];   // staged offset of each halo cell, exclusive prefix
-  int start[kHaloMax];     // the cell's first index in sorted_point_idx
+  int off[Cfg::kHaloMax + 1];  // staged offset of each halo cell, exclusive prefix
+  int start[Cfg::kHaloMax];    // the cell's first index in sorted_point_idx
   int warp_tot[kThreads / 32];
   int next_unit;            // next work unit of the tile (see process_tile)
   unsigned kept[kMaskWords][kThreads];  // per thread: window positions pass A accepted
@@ -117,9 +124,11 @@ struct Stage {
 // kBlocks CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
 template <class Cfg>
 constexpr bool fits_sm() {
-  return Cfg::kBlocks * (sizeof(Stage<Cfg::kCap>) + 16 + 1024) <= 228 * 1024;
+  return Cfg::kBlocks * (sizeof(Stage<Cfg>) + 16 + 1024) <= 228 * 1024 && Cfg::kItemsPerTile <= kMaxItemsPerTile &&
+         Cfg::kHaloMax <= kCellsPerThread * kThreads;
 }
-static_assert(fits_sm<Cfg2560x4>() && fits_sm<Cfg3712x3>() && fits_sm<Cfg5888x2>(),
+static_assert(fits_sm<Cfg2560x4>() && fits_sm<Cfg3712x3>() && fits_sm<Cfg5888x2>() && fits_sm<Cfg2560x4Sq>() &&
+                  fits_sm<Cfg3712x3Sq>(),
               "a stage configuration exceeds the shared memory of its blocks per SM");
 
 // Clipped bucket range of a hash entry: [x, x + count) within [0, n_sorted).
@@ -129,10 +138,10 @@ __device__ __forceinline__ int2 bucket_range(int2 h, int n_sorted) {
 }
 
 // Candidates from the tile's shared-memory stage.
-template <int kCap>
+template <class Cfg>
 struct SrcStaged {
   static constexpr bool kStaged = true;
-  const Stage<kCap>* st;
+  const Stage<Cfg>* st;
   int rv0, ru0, nu;
   __device__ __forceinline__ int cell(int vv, int uu) const { return (vv - rv0) * nu + (uu - ru0); }
   __device__ __forceinline__ int2 range(const SampleArgs&, int vv, int uu) const {
@@ -1013,7 +1022,7 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
 // around them.
 struct Sched {
   int* work;    // [max items] estimated cost
-  int* item;    // [max items] (tile << 8) | (first row << 4) | rows
+  int* item;    // [max items] item_code(tile, first row, rows)
   int* cols;    // [max items] (first column << 8) | end column, within the tile
   int* view;    // [max items] view of the item (batched launches; else null)
   int* order;   // [max items] item indices, heaviest first
@@ -1025,11 +1034,20 @@ struct Sched {
 
 __device__ __forceinline__ int cost_class(int w) { return 31 - __clz(w | 1); }
 
+// A work item: tile t (< 2^21, local to its view), first row and row count
+// (<= 16) within the tile.
+__host__ __device__ constexpr int item_code(int t, int row, int rows) { return (t << 10) | (row << 5) | rows; }
+__device__ __forceinline__ int item_tile(int it) { return it >> 10; }
+__device__ __forceinline__ int item_row(int it) { return (it >> 5) & 31; }
+__device__ __forceinline__ int item_rows(int it) { return it & 31; }
+constexpr int64_t kMaxTilesPerView = 1 << 21;
+
 // Items of tile t (local to its view) of an H x W image, appended to the queue.
-// The clipped point counts of the tile's whole window halo (up to 12 rows x
-// 36 columns) are loaded once, two columns per lane; the halo of any row band
-// or column range of the tile is a sub-rectangle of it, summed from those
-// registers with one warp reduction.
+// The clipped point counts of the tile's whole window halo (up to
+// (kTileH + 4) rows x (kTileW + 4) columns) are loaded once, up to two columns
+// per lane; the halo of any row band or column range of the tile is a
+// sub-rectangle of it, summed from those registers with one warp reduction.
+template <int kTileH, int kTileW>
 __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k, int tiles_x,
                                           int t, int view, int cap, Sched& sc) {
   constexpr int kHaloRows = kTileH + kMaxKernel - 1;
@@ -1091,7 +1109,7 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
         const int w = hs > cap ? c * 4 : c;
         const int i = atomicAdd(sc.n_items, 1);
         sc.work[i] = w;
-        sc.item[i] = (t << 8) | ((vb - v0) << 4) | rows;
+        sc.item[i] = item_code(t, vb - v0, rows);
         sc.cols[i] = (c0 << 8) | c1;
         if (sc.view) sc.view[i] = view;
         atomicAdd(sc.counts + (sc.view ? view * 32 : 0) + cost_class(w), 1);
@@ -1114,11 +1132,12 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
   }
 }
 
+template <int kTileH, int kTileW>
 __global__ void __launch_bounds__(256) k_tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k,
                                                    int tiles_x, int ntiles, int cap, Sched sc) {
   const int t = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (t >= ntiles) return;
-  tile_work(hash, n_sorted, H, W, k, tiles_x, t, 0, cap, sc);
+  tile_work<kTileH, kTileW>(hash, n_sorted, H, W, k, tiles_x, t, 0, cap, sc);
 }
 
 __global__ void __launch_bounds__(256) k_tile_order(Sched sc) {
@@ -1177,10 +1196,13 @@ __global__ void __launch_bounds__(256) k_batch_order_place(Sched sc, const int* 
 }
 
 // Rays of rows [v0, v0 + rows) and tile columns [c0, c1) of the tile at u0
-// (u0 + c0 < width).
-template <int kCap>
-__device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<kCap>& st, int v0, int rows, int u0,
-                                             int c0 = 0, int c1 = kTileW) {
+// (u0 + c0 < width).  Thread tid is tile pixel (tid / kTileW, tid % kTileW);
+// a ray is named by that pixel index in the rank order.
+template <class Cfg>
+__device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<Cfg>& st, int v0, int rows, int u0, int c0,
+                                             int c1) {
+  constexpr int kTileW = Cfg::kTileW;
+  constexpr int kCap = Cfg::kCap;
   const int W = a.cam.width, H = a.cam.height, k = a.opt.k;
   const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
   const int rv0 = max(0, v0 - lo), rv1 = min(H - 1, v0 + rows - 1 + hi);
@@ -1252,9 +1274,10 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<kCap>& s
   // unit of its total work divided by its warps.
   int nheavy, nvalid;
   {
-    const int pu = u0 + (tid & 31), pv = v0 + (tid >> 5);
+    const int col = tid % kTileW, row = tid / kTileW;
+    const int pu = u0 + col, pv = v0 + row;
     int T = -1;  // window candidates; -1: no ray at this pixel
-    if (pu < W && pv < H && (tid >> 5) < rows && (tid & 31) >= c0 && (tid & 31) < c1) {
+    if (pu < W && pv < H && row < rows && col >= c0 && col < c1) {
       T = 0;
       if (staged && pu - lo >= 0 && pu + hi <= W - 1) {
         // unclamped columns: each window row is a run of k consecutive halo cells
@@ -1266,7 +1289,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<kCap>& s
         for (int l = 0; l < k * k; l++) {
           int vv, uu;
           window_cell(pv, pu, k, H, W, l, vv, uu);
-          const int2 rg = staged ? SrcStaged<kCap>{&st, rv0, ru0, nu}.range(a, vv, uu) : SrcGlobal{}.range(a, vv, uu);
+          const int2 rg = staged ? SrcStaged<Cfg>{&st, rv0, ru0, nu}.range(a, vv, uu) : SrcGlobal{}.range(a, vv, uu);
           T += rg.y - rg.x;
         }
       }
@@ -1306,9 +1329,9 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<kCap>& s
       if (rk < nvalid) {
         const int px = st.order[rk];
         if (staged)
-          sample_ray(a, SrcStaged<kCap>{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31), &st.kept[0][tid]);
+          sample_ray(a, SrcStaged<Cfg>{&st, rv0, ru0, nu}, v0 + px / kTileW, u0 + px % kTileW, &st.kept[0][tid]);
         else
-          sample_ray(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31), nullptr);
+          sample_ray(a, SrcGlobal{}, v0 + px / kTileW, u0 + px % kTileW, nullptr);
       }
       continue;
     }
@@ -1316,9 +1339,9 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<kCap>& s
     if (h >= nheavy) break;
     const int px = st.order[h];
     if (staged)
-      sample_ray_warp(a, SrcStaged<kCap>{&st, rv0, ru0, nu}, v0 + (px >> 5), u0 + (px & 31));
+      sample_ray_warp(a, SrcStaged<Cfg>{&st, rv0, ru0, nu}, v0 + px / kTileW, u0 + px % kTileW);
     else
-      sample_ray_warp(a, SrcGlobal{}, v0 + (px >> 5), u0 + (px & 31));
+      sample_ray_warp(a, SrcGlobal{}, v0 + px / kTileW, u0 + px % kTileW);
   }
   __syncthreads();  // the stage is reused by the next tile
 }
@@ -1326,7 +1349,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<kCap>& s
 template <class Cfg>
 __global__ void __launch_bounds__(kThreads, Cfg::kBlocks) k_quick_sampling(SampleArgs a, Sched sc, int tiles_x) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Stage<Cfg::kCap>& st = *reinterpret_cast<Stage<Cfg::kCap>*>(smem_raw);
+  Stage<Cfg>& st = *reinterpret_cast<Stage<Cfg>*>(smem_raw);
   __shared__ int s_next;
   const int n = *sc.n_items;
   for (;;) {
@@ -1336,9 +1359,9 @@ __global__ void __launch_bounds__(kThreads, Cfg::kBlocks) k_quick_sampling(Sampl
     if (i >= n) break;
     const int j = sc.order[i];
     const int it = sc.item[j], cc = sc.cols[j];
-    const int t = it >> 8;
-    process_tile(a, st, (t / tiles_x) * kTileH + ((it >> 4) & 15), it & 15, (t % tiles_x) * kTileW, cc >> 8,
-                 cc & 255);
+    const int t = item_tile(it);
+    process_tile(a, st, (t / tiles_x) * Cfg::kTileH + item_row(it), item_rows(it), (t % tiles_x) * Cfg::kTileW,
+                 cc >> 8, cc & 255);
   }
 }
 
@@ -1352,7 +1375,7 @@ __global__ void __launch_bounds__(kThreads, Cfg::kBlocks) k_quick_sampling(Sampl
 // each view (exclusive scan; tile_base[n_views] = all tiles).  One warp.
 // Also the first packed-point slot of each view (pack_base; regions padded to
 // 16 slots) and the views' packed-point arrays inside `pts`.
-__global__ void k_batch_setup(const hp_view* __restrict__ views, int n_views, int heavy,
+__global__ void k_batch_setup(const hp_view* __restrict__ views, int n_views, int heavy, int tile_h, int tile_w,
                               SampleArgs* __restrict__ args, int* __restrict__ tile_base, int* __restrict__ pack_base,
                               float4* __restrict__ pts) {
   const int lane = threadIdx.x;
@@ -1400,7 +1423,7 @@ __global__ void k_batch_setup(const hp_view* __restrict__ views, int n_views, in
       a.mask = hv.mask;
       a.heavy = heavy;
       args[v] = a;
-      tiles = ((hv.cam.width + kTileW - 1) / kTileW) * ((hv.cam.height + kTileH - 1) / kTileH);
+      tiles = ((hv.cam.width + tile_w - 1) / tile_w) * ((hv.cam.height + tile_h - 1) / tile_h);
     }
     int incl = tiles;
 #pragma unroll
@@ -1443,6 +1466,7 @@ __global__ void k_batch_pack(const SampleArgs* __restrict__ args, const int* __r
 }
 
 // One warp per global tile: find its view, then queue the tile's items.
+template <int kTileH, int kTileW>
 __global__ void __launch_bounds__(256) k_batch_tile_work(const SampleArgs* __restrict__ args,
                                                          const int* __restrict__ tile_base, int n_views,
                                                          int total_tiles, int cap, Sched sc) {
@@ -1458,7 +1482,8 @@ __global__ void __launch_bounds__(256) k_batch_tile_work(const SampleArgs* __res
   }
   const SampleArgs& a = args[lo];
   const int tiles_x = (a.cam.width + kTileW - 1) / kTileW;
-  tile_work(a.hash, a.n_sorted, a.cam.height, a.cam.width, a.opt.k, tiles_x, g - tile_base[lo], lo, cap, sc);
+  tile_work<kTileH, kTileW>(a.hash, a.n_sorted, a.cam.height, a.cam.width, a.opt.k, tiles_x, g - tile_base[lo], lo,
+                            cap, sc);
 }
 
 // The persistent sampling kernel over the batch's queue; each item's view
@@ -1467,7 +1492,7 @@ template <class Cfg>
 __global__ void __launch_bounds__(kThreads, Cfg::kBlocks)
     k_quick_sampling_batch(const SampleArgs* __restrict__ args, Sched sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Stage<Cfg::kCap>& st = *reinterpret_cast<Stage<Cfg::kCap>*>(smem_raw);
+  Stage<Cfg>& st = *reinterpret_cast<Stage<Cfg>*>(smem_raw);
   __shared__ int s_next;
   __shared__ SampleArgs s_args;
   const int n = *sc.n_items;
@@ -1480,10 +1505,10 @@ __global__ void __launch_bounds__(kThreads, Cfg::kBlocks)
     if (threadIdx.x == 0) s_args = args[sc.view[j]];
     __syncthreads();
     const int it = sc.item[j], cc = sc.cols[j];
-    const int t = it >> 8;
-    const int tiles_x = (s_args.cam.width + kTileW - 1) / kTileW;
-    process_tile(s_args, st, (t / tiles_x) * kTileH + ((it >> 4) & 15), it & 15, (t % tiles_x) * kTileW, cc >> 8,
-                 cc & 255);
+    const int t = item_tile(it);
+    const int tiles_x = (s_args.cam.width + Cfg::kTileW - 1) / Cfg::kTileW;
+    process_tile(s_args, st, (t / tiles_x) * Cfg::kTileH + item_row(it), item_rows(it), (t % tiles_x) * Cfg::kTileW,
+                 cc >> 8, cc & 255);
   }
 }
 
@@ -1497,21 +1522,49 @@ __global__ void k_ray_directions(DevCamera cam, float* __restrict__ dirs) {
   dirs[3 * (size_t)p + 2] = r.d[2];
 }
 
-// The sampling kernels of each stage configuration.
+// The kernels and shapes of each stage configuration.
 struct SamplingKernels {
   void (*view)(SampleArgs, Sched, int);
   void (*batch)(const SampleArgs*, Sched);
+  void (*tile_work)(const int2*, int, int, int, int, int, int, int, Sched);
+  void (*batch_tile_work)(const SampleArgs*, const int*, int, int, int, Sched);
   size_t smem;
-  int cap;
+  int cap, blocks, tile_h, tile_w, items_per_tile;
 };
 template <class Cfg>
 static SamplingKernels sampling_kernels() {
-  return {k_quick_sampling<Cfg>, k_quick_sampling_batch<Cfg>, sizeof(Stage<Cfg::kCap>), Cfg::kCap};
+  return {k_quick_sampling<Cfg>,
+          k_quick_sampling_batch<Cfg>,
+          k_tile_work<Cfg::kTileH, Cfg::kTileW>,
+          k_batch_tile_work<Cfg::kTileH, Cfg::kTileW>,
+          sizeof(Stage<Cfg>),
+          Cfg::kCap,
+          Cfg::kBlocks,
+          Cfg::kTileH,
+          Cfg::kTileW,
+          Cfg::kItemsPerTile};
 }
 static const SamplingKernels& stage_kernels(int config) {  // config 1..kStageConfigs
   static const SamplingKernels table[kStageConfigs] = {sampling_kernels<Cfg2560x4>(), sampling_kernels<Cfg3712x3>(),
-                                                       sampling_kernels<Cfg5888x2>()};
+                                                       sampling_kernels<Cfg5888x2>(), sampling_kernels<Cfg2560x4Sq>(),
+                                                       sampling_kernels<Cfg3712x3Sq>()};
   return table[config - 1];
+}
+
+static int64_t tiles_of(int64_t H, int64_t W, int tile_h, int tile_w) {
+  return ((W + tile_w - 1) / tile_w) * ((H + tile_h - 1) / tile_h);
+}
+
+// Schedule entries an H x W view can need under any configuration (workspaces
+// are sized for the largest, so one workspace serves every tuning).
+static int64_t max_view_items(int64_t H, int64_t W) {
+  int64_t m = 0;
+  for (int c = 1; c <= kStageConfigs; c++) {
+    const SamplingKernels& K = stage_kernels(c);
+    const int64_t items = tiles_of(H, W, K.tile_h, K.tile_w) * K.items_per_tile;
+    if (items > m) m = items;
+  }
+  return m;
 }
 
 // The stage exceeds the 48 KB default of dynamic shared memory: opt the
@@ -1567,10 +1620,9 @@ struct SchedLayout {
   size_t work, item, cols, order, view, small, pts, total;
 };
 
-// up to kItemsPerTile items per tile (every row its own item, in quarters)
+// up to items_per_tile items per tile (every row its own item, in quarters)
 static SchedLayout sched_layout(int64_t H, int64_t W, int64_t n_sorted) {
-  const int64_t ntiles = ((W + kTileW - 1) / kTileW) * ((H + kTileH - 1) / kTileH);
-  const size_t per = align256s(sizeof(int) * (size_t)(ntiles * kItemsPerTile));
+  const size_t per = align256s(sizeof(int) * (size_t)max_view_items(H, W));
   SchedLayout L;
   L.work = 0;
   L.item = per;
@@ -1590,9 +1642,9 @@ struct BatchLayout {
   size_t args, tile_base, pack_base, views, buckets, pts, total;
 };
 
-static BatchLayout batch_layout(int64_t total_tiles, int n_views, int64_t total_slots) {
+static BatchLayout batch_layout(int64_t total_items, int n_views, int64_t total_slots) {
   BatchLayout B;
-  const size_t per = align256s(sizeof(int) * (size_t)(total_tiles * kItemsPerTile));
+  const size_t per = align256s(sizeof(int) * (size_t)total_items);
   B.q.work = 0;
   B.q.item = per;
   B.q.cols = 2 * per;
@@ -1667,6 +1719,9 @@ static int32_t check_sampling(const char* who, const float* xyz, int64_t n_point
     return set_error(HP_ERR_INVALID_ARGUMENT, "%s: num_sample_points_per_ray and num_point_cloud_per_sp must be >= 1",
                      who);
   const int64_t hw = (int64_t)cam->height * cam->width;
+  if (tiles_of(cam->height, cam->width, 16, 16) >= kMaxTilesPerView ||
+      tiles_of(cam->height, cam->width, 8, 32) >= kMaxTilesPerView)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "%s: image too large (%lld pixels)", who, (long long)hw);
   if (hw * opt->num_sample_points_per_ray * (int64_t)(opt->num_point_cloud_per_sp > 3 ? opt->num_point_cloud_per_sp : 3) >=
       (1ll << 40))
     return set_error(HP_ERR_INVALID_ARGUMENT, "%s: output too large", who);
@@ -1677,6 +1732,20 @@ static int32_t check_sampling(const char* who, const float* xyz, int64_t n_point
     return set_error(HP_ERR_INVALID_ARGUMENT, "%s: null pointer", who);
   if (((uintptr_t)hash_table & 7) != 0)
     return set_error(HP_ERR_INVALID_ARGUMENT, "%s: hash_table must be 8-byte aligned", who);
+  return HP_OK;
+}
+
+extern "C" int32_t hp_stage_config_info(int32_t config, int32_t* tile_h, int32_t* tile_w, int32_t* stage_points,
+                                        int32_t* blocks_per_sm) {
+  if (config == 0) config = 1;
+  if (config < 1 || config > kStageConfigs)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_stage_config_info: stage_config %d outside 0..%d", config,
+                     kStageConfigs);
+  const SamplingKernels& K = stage_kernels(config);
+  if (tile_h) *tile_h = K.tile_h;
+  if (tile_w) *tile_w = K.tile_w;
+  if (stage_points) *stage_points = K.cap;
+  if (blocks_per_sm) *blocks_per_sm = K.blocks;
   return HP_OK;
 }
 
@@ -1712,8 +1781,8 @@ extern "C" int32_t hp_quick_sampling_tuned(const float* xyz, int64_t n_points, c
   if (int32_t rc = sampling_grid(tn.config, &blocks, &sms)) return rc;
   if (tn.per_sm > 0 && tn.per_sm * sms < blocks) blocks = tn.per_sm * sms;
   const SamplingKernels& K = stage_kernels(tn.config);
-  const int tiles_x = (cam->width + kTileW - 1) / kTileW;
-  const int ntiles = tiles_x * ((cam->height + kTileH - 1) / kTileH);
+  const int tiles_x = (cam->width + K.tile_w - 1) / K.tile_w;
+  const int ntiles = (int)tiles_of(cam->height, cam->width, K.tile_h, K.tile_w);
   char* ws = (char*)workspace;
   Sched sc;
   sc.work = (int*)(ws + L.work);
@@ -1733,13 +1802,13 @@ extern "C" int32_t hp_quick_sampling_tuned(const float* xyz, int64_t n_points, c
                                                                       (int)n_points, (float4*)(ws + L.pts));
     if (int32_t rc = check_launch("k_pack_points")) return rc;
   }
-  k_tile_work<<<(ntiles + 7) / 8, 256, 0, st>>>(a.hash, a.n_sorted, cam->height, cam->width, opt->kernel_size, tiles_x,
+  K.tile_work<<<(ntiles + 7) / 8, 256, 0, st>>>(a.hash, a.n_sorted, cam->height, cam->width, opt->kernel_size, tiles_x,
                                                  ntiles, K.cap, sc);
   if (int32_t rc = check_launch("k_tile_work")) return rc;
   k_tile_order<<<(ntiles + 255) / 256 < 148 ? (ntiles + 255) / 256 : 148, 256, 0, st>>>(sc);
   if (int32_t rc = check_launch("k_tile_order")) return rc;
-  // a split tile yields up to kItemsPerTile items: size the persistent grid by those, not by tiles
-  const int64_t max_items = (int64_t)ntiles * kItemsPerTile;
+  // a split tile yields up to items_per_tile items: size the persistent grid by those, not by tiles
+  const int64_t max_items = (int64_t)ntiles * K.items_per_tile;
   K.view<<<blocks < max_items ? blocks : (int)max_items, kThreads, K.smem, st>>>(a, sc, tiles_x);
   return check_launch("k_quick_sampling");
 }
@@ -1759,18 +1828,28 @@ static int64_t batch_slots(const hp_view* views, int32_t n_views) {
   return total;
 }
 
-static int64_t batch_tiles(const hp_view* views, int32_t n_views) {
+static int64_t batch_tiles(const hp_view* views, int32_t n_views, int tile_h, int tile_w) {
   int64_t total = 0;
-  for (int32_t v = 0; v < n_views; v++)
-    total += (int64_t)((views[v].cam.width + kTileW - 1) / kTileW) * ((views[v].cam.height + kTileH - 1) / kTileH);
+  for (int32_t v = 0; v < n_views; v++) total += tiles_of(views[v].cam.height, views[v].cam.width, tile_h, tile_w);
   return total;
+}
+
+// Schedule entries a batch can need under any configuration.
+static int64_t batch_max_items(const hp_view* views, int32_t n_views) {
+  int64_t m = 0;
+  for (int c = 1; c <= kStageConfigs; c++) {
+    const SamplingKernels& K = stage_kernels(c);
+    const int64_t items = batch_tiles(views, n_views, K.tile_h, K.tile_w) * K.items_per_tile;
+    if (items > m) m = items;
+  }
+  return m;
 }
 
 extern "C" size_t hp_quick_sampling_batch_workspace_size(const hp_view* views, int32_t n_views) {
   if (!views || n_views <= 0) return 0;
   for (int32_t v = 0; v < n_views; v++)
     if (views[v].cam.width <= 0 || views[v].cam.height <= 0 || views[v].n_sorted < 0) return 0;
-  return batch_layout(batch_tiles(views, n_views), n_views, batch_slots(views, n_views)).total;
+  return batch_layout(batch_max_items(views, n_views), n_views, batch_slots(views, n_views)).total;
 }
 
 extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* views_device, int32_t n_views,
@@ -1789,11 +1868,11 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
       return set_error(rc, "%s (view %d)", msg, v);
     }
   }
-  const int64_t total_tiles = batch_tiles(views, n_views);
+  const int64_t max_items = batch_max_items(views, n_views);
   const int64_t total_slots = batch_slots(views, n_views);
-  if (total_tiles * kItemsPerTile >= (1ll << 31) || total_slots >= (1ll << 31))
+  if (max_items >= (1ll << 31) || total_slots >= (1ll << 31))
     return set_error(HP_ERR_INVALID_ARGUMENT, "%s: too many tiles or points in one batch", who);
-  const BatchLayout B = batch_layout(total_tiles, n_views, total_slots);
+  const BatchLayout B = batch_layout(max_items, n_views, total_slots);
   if (!workspace || workspace_bytes < B.total || ((uintptr_t)workspace & 255) != 0)
     return set_error(HP_ERR_WORKSPACE, "%s: workspace needs %zu bytes, 256-byte aligned (got %zu)", who, B.total,
                      workspace_bytes);
@@ -1801,6 +1880,7 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
   if (int32_t rc = sampling_grid(tn.config, &blocks, &sms)) return rc;
   if (tn.per_sm > 0 && tn.per_sm * sms < blocks) blocks = tn.per_sm * sms;
   const SamplingKernels& K = stage_kernels(tn.config);
+  const int64_t total_tiles = batch_tiles(views, n_views, K.tile_h, K.tile_w);
   char* ws = (char*)workspace;
   cudaStream_t st = (cudaStream_t)stream;
   if (!views_device) {  // copy the table into the workspace
@@ -1827,21 +1907,22 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
       cudaMemsetAsync(ws + B.buckets, 0, 2 * bucket_bytes, st) != cudaSuccess)
     return set_error(HP_ERR_CUDA, "%s: memset failed", who);
   int* pack_base = (int*)(ws + B.pack_base);
-  k_batch_setup<<<1, 32, 0, st>>>(views_device, n_views, tn.heavy, args, tile_base, pack_base, (float4*)(ws + B.pts));
+  k_batch_setup<<<1, 32, 0, st>>>(views_device, n_views, tn.heavy, K.tile_h, K.tile_w, args, tile_base, pack_base,
+                                  (float4*)(ws + B.pts));
   if (int32_t rc = check_launch("k_batch_setup")) return rc;
   if (total_slots > 0) {
     k_batch_pack<<<(unsigned)((total_slots + 255) / 256), 256, 0, st>>>(args, pack_base, n_views, (int)total_slots);
     if (int32_t rc = check_launch("k_batch_pack")) return rc;
   }
   const int nt = (int)total_tiles;
-  k_batch_tile_work<<<(nt + 7) / 8, 256, 0, st>>>(args, tile_base, n_views, nt, K.cap, sc);
+  K.batch_tile_work<<<(nt + 7) / 8, 256, 0, st>>>(args, tile_base, n_views, nt, K.cap, sc);
   if (int32_t rc = check_launch("k_batch_tile_work")) return rc;
   k_batch_order_scan<<<1, 1024, 0, st>>>(sc, n_views, base);
   if (int32_t rc = check_launch("k_batch_order_scan")) return rc;
   k_batch_order_place<<<(nt + 255) / 256 < 148 ? (nt + 255) / 256 : 148, 256, 0, st>>>(sc, base);
   if (int32_t rc = check_launch("k_batch_order_place")) return rc;
-  const int64_t max_items = (int64_t)nt * kItemsPerTile;
-  K.batch<<<blocks < max_items ? blocks : (int)max_items, kThreads, K.smem, st>>>(args, sc);
+  const int64_t grid_items = (int64_t)nt * K.items_per_tile;
+  K.batch<<<blocks < grid_items ? blocks : (int)grid_items, kThreads, K.smem, st>>>(args, sc);
   return check_launch("k_quick_sampling_batch");
 }
 

@@ -12,7 +12,7 @@ import ctypes
 import torch
 
 from . import native
-from .ops import make_options
+from .ops import make_options, make_tuning
 
 _vp = ctypes.c_void_p
 
@@ -78,6 +78,33 @@ class ViewPipeline:
             ctypes.byref(self.tuning) if self.tuning is not None else None, _vp(self.ws_sample.data_ptr()),
             self.ws_sample_bytes, _vp(stream.cuda_stream))
         native.check(rc, "hp_quick_sampling")
+
+    def tune(self, xyz, cams, stream=None, reps=2):
+        """Pick the fastest stage configuration of the sampling kernel (hp_tuning.stage_config) for
+        this shape on the given views, timed with CUDA events; outputs never depend on it.  Returns
+        the configuration, which later sample() calls use."""
+        import torch
+        stream = stream or torch.cuda.current_stream(self.device)
+        best = None
+        for cfg in native.STAGE_CONFIGS:
+            self.tuning = make_tuning(stage_config=cfg)
+            ms = []
+            for rep in range(reps + 1):
+                tot = 0.0
+                for cam in cams:
+                    self.build(xyz, cam, stream)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    self.sample(xyz, cam, stream)
+                    e1.record(stream)
+                    e1.synchronize()
+                    tot += e0.elapsed_time(e1)
+                if rep:  # the first pass loads and warms the configuration's kernels
+                    ms.append(tot)
+            if best is None or min(ms) < best[0]:
+                best = (min(ms), cfg)
+        self.tuning = make_tuning(stage_config=best[1])
+        return best[1]
 
     def render(self, xyz, cam, stream=None):
         stream = stream or torch.cuda.current_stream(self.device)

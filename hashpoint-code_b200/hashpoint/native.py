@@ -40,7 +40,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
 # C-ABI symbols declared in include/hashpoint_b200.h
 EXPORTS = ["hp_version", "hp_last_error", "hp_projection_rounding", "hp_pts2plane_workspace_size", "hp_pts2plane",
            "hp_pts2plane_noalloc", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling",
-           "hp_quick_sampling_tuned",
+           "hp_quick_sampling_tuned", "hp_stage_config_info",
            "hp_quick_sampling_batch_workspace_size", "hp_quick_sampling_batch", "hp_quick_query_for_nearby_point",
            "hp_scatter", "hp_ray_directions", "hp_mask_scan", "hp_mask_scan_workspace_size", "hp_feature_query",
            "hp_clamp_t", "hp_render", "hp_aggregator_packed_size", "hp_aggregator_pack",
@@ -183,7 +183,15 @@ class HpTuning(ctypes.Structure):
     _fields_ = [("heavy_window", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("stage_config", ctypes.c_int32)]
 
 
-STAGE_CONFIGS = (1, 2, 3)  # hp_tuning.stage_config values
+STAGE_CONFIGS = (1, 2, 3, 4, 5)  # hp_tuning.stage_config values (see include/hashpoint_b200.h)
+
+
+def stage_config_info(config):
+    """{tile_h, tile_w, stage_points, blocks_per_sm} of a stage configuration (hp_stage_config_info)."""
+    L = lib()
+    v = [ctypes.c_int32() for _ in range(4)]
+    check(L.hp_stage_config_info(int(config), *[ctypes.byref(x) for x in v]), "hp_stage_config_info", L)
+    return dict(zip(("tile_h", "tile_w", "stage_points", "blocks_per_sm"), (x.value for x in v)))
 
 
 class HpView(ctypes.Structure):
@@ -231,6 +239,9 @@ def lib():
         L.hp_quick_sampling_tuned.argtypes = [vp, i64, cam_p, opt_p, vp, i64, vp, vp, vp, vp, vp,
                                               ctypes.POINTER(HpTuning), vp, sz, vp]
         L.hp_quick_sampling_tuned.restype = i32
+        ip = ctypes.POINTER(ctypes.c_int32)
+        L.hp_stage_config_info.argtypes = [i32, ip, ip, ip, ip]
+        L.hp_stage_config_info.restype = i32
         view_p = ctypes.POINTER(HpView)
         L.hp_quick_sampling_batch_workspace_size.argtypes = [view_p, i32]
         L.hp_quick_sampling_batch_workspace_size.restype = sz

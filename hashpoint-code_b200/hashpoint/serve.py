@@ -17,6 +17,13 @@ resolution) -- arrive over time.  The loop
     freed) and records each request's latency from its arrival to its
     batch's completion on the GPU.
 
+The host work per batch is kept small and free of allocation: output buffers
+come from a pool per resolution, each in-flight slot owns a workspace that
+only grows, and every cached hash table carries its hp_view template (only the
+output pointers are filled in per request).  The loop spins on its events and
+the next arrival for the last stretch before either is due instead of
+sleeping through it, so a request is noticed within microseconds.
+
 Each request's outputs are exactly those of a plain per-view launch: the batch
 runs the same per-ray code, and a hash table is the same whether built for the
 request or found in the cache.
@@ -61,7 +68,8 @@ def camera_for(pose_c2w, width, height, f_at_800=1111.0):
 
 
 class _Entry:
-    """A cached hash table: (scene, pose, width, height) -> sorted ids, depths, table."""
+    """A cached hash table: (scene, pose, width, height) -> sorted ids, depths, table, and the
+    hp_view of a request for it (output pointers left to fill)."""
 
     def __init__(self, n, H, W, device):
         self.sidx = torch.empty(n, dtype=torch.int32, device=device)
@@ -70,6 +78,7 @@ class _Entry:
         self.ready = None  # event recorded after the build
         self.bytes = 8 * n + 8 * H * W
         self.users = 0     # in-flight batches that read it
+        self.view = None   # native.HpView template
 
 
 class SceneStore:
@@ -84,6 +93,8 @@ class SceneStore:
         self.cams = {}
         self.scene_bytes = sum(12 * c.shape[0] for c in self.clouds)
         self.bytes = self.scene_bytes  # scenes + cached tables
+        self.hits = 0    # lookups served from the cache
+        self.misses = 0  # lookups that built a table
 
     def camera(self, scene, pose, width, height):
         key = (scene, pose, width, height)
@@ -126,12 +137,14 @@ class SceneStore:
         key = (req.scene, req.pose, req.width, req.height)
         e = self.cache.get(key)
         if e is not None:
+            self.hits += 1
             self.cache.move_to_end(key)
             if not req.reserved:
                 e.users += 1
             if e.ready is not None:
                 stream.wait_event(e.ready)
             return e
+        self.misses += 1
         xyz = self.clouds[req.scene]
         n = xyz.shape[0]
         cam, c2w, w2c, K = self.camera(req.scene, req.pose, req.width, req.height)
@@ -148,6 +161,8 @@ class SceneStore:
         e.ready = torch.cuda.Event()
         e.ready.record(stream)
         e.users = 1
+        e.view = ops.make_view(xyz, c2w, cam.fx, cam.fy, cam.cx, cam.cy, req.width, req.height, self.options, e.sidx,
+                               e.hash, (None, None, None, None))
         self.cache[key] = e
         self.bytes += e.bytes
         return e
@@ -161,6 +176,21 @@ def output_bytes(req, opt):
 class _Batch:
     def __init__(self, reqs, slot, stream, done, hold):
         self.reqs, self.slot, self.stream, self.done, self.hold = reqs, slot, stream, done, hold
+
+
+class OutputPool:
+    """Reusable quick_sampling output buffers per resolution (sp_xyz, pc_idx, sp_t, mask)."""
+
+    def __init__(self, options, device):
+        self.options, self.device = options, device
+        self.free = collections.defaultdict(list)
+
+    def take(self, width, height):
+        lst = self.free[(width, height)]
+        return lst.pop() if lst else ops.sampling_outputs(height, width, self.options, self.device)
+
+    def give(self, width, height, out):
+        self.free[(width, height)].append(out)
 
 
 class Server:
@@ -182,6 +212,9 @@ class Server:
         self.tuning = tuning if tuning is not None else ops.make_tuning()
         self.out_bytes = 0
         self.batches = 0
+        self.pool = OutputPool(store.options, self.device)
+        self.ws = [None] * len(self.streams)  # workspace per slot (grows, never shrinks)
+        self.tables = [(native.HpView * self.max_views)() for _ in self.streams]
 
     def _bytes_needed(self, req):
         return output_bytes(req, self.store.options) + self.store.entry_bytes(req)
@@ -190,26 +223,26 @@ class Server:
         # heavy views first: the batch takes its views' tiles in table order
         reqs = sorted(reqs, key=lambda r: -self.store.clouds[r.scene].shape[0])
         s = self.streams[slot]
-        opt = self.store.options
-        hold = []  # tensors that must live until the batch is done
-        views = []
+        hold = []  # cached tables the batch reads
+        table = self.tables[slot]
+        n = len(reqs)
         with torch.cuda.stream(s):
-            for r in reqs:
-                e = self.store.lookup(r, s, lambda n: torch.empty(max(n, 1), dtype=torch.uint8, device=self.device))
-                cam, c2w, _, _ = self.store.camera(r.scene, r.pose, r.width, r.height)
-                out = ops.sampling_outputs(r.height, r.width, opt, self.device)
+            for i, r in enumerate(reqs):
+                e = self.store.lookup(r, s, lambda b: torch.empty(max(b, 1), dtype=torch.uint8, device=self.device))
+                out = self.pool.take(r.width, r.height)
                 r.outputs = out
-                views.append(ops.make_view(self.store.clouds[r.scene], c2w, cam.fx, cam.fy, cam.cx, cam.cy,
-                                           r.width, r.height, opt, e.sidx, e.hash, out))
+                table[i] = e.view
+                v = table[i]  # shares the table's memory
+                v.sp_xyz, v.pc_idx, v.sp_t, v.mask = (out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(),
+                                                      out[3].data_ptr())
                 hold.append(e)
                 r.status = "running"
-            n = len(views)
-            table = (native.HpView * n)(*views)
             L = native.lib()
             ws_bytes = L.hp_quick_sampling_batch_workspace_size(table, n)
-            ws = torch.empty(ws_bytes, dtype=torch.uint8, device=self.device)
-            hold.append(ws)
-            rc = L.hp_quick_sampling_batch(table, None, n, ctypes.byref(self.tuning), _vp(ws.data_ptr()), ws_bytes,
+            ws = self.ws[slot]
+            if ws is None or ws.numel() < ws_bytes:
+                ws = self.ws[slot] = torch.empty(ws_bytes, dtype=torch.uint8, device=self.device)
+            rc = L.hp_quick_sampling_batch(table, None, n, ctypes.byref(self.tuning), _vp(ws.data_ptr()), ws.numel(),
                                            _vp(s.cuda_stream))
             native.check(rc, "hp_quick_sampling_batch")
             done = torch.cuda.Event(enable_timing=True)
@@ -228,13 +261,16 @@ class Server:
             if self.on_result is not None:
                 self.on_result(r)
             self.out_bytes -= output_bytes(r, self.store.options)
+            self.pool.give(r.width, r.height, r.outputs)
             r.outputs = None
         self.free_slots.append(b.slot)
 
-    def run(self, requests, poll_s=50e-6, time_limit_s=600.0):
+    def run(self, requests, poll_s=200e-6, time_limit_s=600.0):
         """Serve `requests` (arrival times relative to the start) in real time; returns stats.
         Python's cyclic garbage collector is paused while the loop runs (a collection pass
-        stalls the launch loop for milliseconds) and restored afterwards."""
+        stalls the launch loop for milliseconds) and restored afterwards.  The loop sleeps
+        only while the next arrival is more than poll_s away and nothing can be launched;
+        otherwise it spins."""
         gc_was = gc.isenabled()
         gc.disable()
         try:
@@ -244,6 +280,7 @@ class Server:
                 gc.enable()
 
     def _run(self, requests, poll_s, time_limit_s):
+        hits0, misses0 = self.store.hits, self.store.misses
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         waiting = collections.deque()
         inflight = []
@@ -287,11 +324,11 @@ class Server:
                 if batch:
                     inflight.append(self._launch(batch, self.free_slots.pop(0), t0_event))
                     continue
-            if inflight and not (waiting and self.free_slots):
-                # nothing to launch: wait briefly for arrivals or completions
-                time.sleep(poll_s)
-            elif not inflight and not waiting and pending:
-                time.sleep(min(poll_s, max(0.0, pending[0].arrival - (time.perf_counter() - t0))))
+            if not inflight and not waiting and pending:
+                # idle until the next arrival: sleep through all but its last poll_s, then spin
+                gap = pending[0].arrival - (time.perf_counter() - t0)
+                if gap > 2 * poll_s:
+                    time.sleep(gap - poll_s)
         torch.cuda.synchronize(self.device)
         done = [r for r in requests if r.status == "done"]
         lat = np.array([r.done_ms - 1e3 * r.arrival for r in done]) if done else np.zeros(0)
@@ -303,7 +340,8 @@ class Server:
             "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
             "mean_ms": float(lat.mean()) if len(lat) else None,
             "rays": rays, "span_ms": span_ms, "rays_per_s": rays / (span_ms * 1e-3) if span_ms > 0 else None,
-            "cache_entries": len(self.store.cache),
+            "cache_entries": len(self.store.cache), "cache_hits": self.store.hits - hits0,
+            "cache_misses": self.store.misses - misses0,
         }
 
 

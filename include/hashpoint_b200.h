@@ -102,7 +102,7 @@ HP_API int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_camera*
  * application embedding it, or a service that must not grow its device
  * footprint after start-up, has no way to provide hp_pts2plane's workspace.
  * This entry point takes the same inputs and outputs and allocates nothing;
- * its scratch is an array built into the library (about 10 MB of device
+ * its scratch is an array built into the library (about 11 MB of device
  * memory on every GPU that loads the library, held until the process exits),
  * so it accepts at most HP_NOALLOC_MAX_POINTS points and HP_NOALLOC_MAX_PIXELS
  * pixels and returns HP_ERR_INVALID_ARGUMENT beyond that.  A call looks up its
@@ -241,9 +241,12 @@ HP_API size_t hp_quick_sampling_workspace_size(int64_t n_sorted, int32_t height,
  *                  whole warp instead of one thread (0..4096; default 320).
  *   blocks_per_sm  resident blocks of the persistent sampling kernel per SM
  *                  (default: as many as fit).
- *   stage_config   shared-memory stage of the sampling kernel (0 = 1):
- *                  1: 2560 staged points per tile, 4 blocks per SM;
- *                  2: 3712 points, 3 blocks per SM;  3: 5888 points, 2 blocks.
+ *   stage_config   stage and tile of the sampling kernel (0 = 1):
+ *                  1: 2560 staged points per tile, 4 blocks per SM, 8 x 32 tiles;
+ *                  2: 3712 points, 3 blocks per SM, 8 x 32;
+ *                  3: 5888 points, 2 blocks per SM, 8 x 32;
+ *                  4: 2560 points, 4 blocks per SM, 16 x 16 tiles;
+ *                  5: 3712 points, 3 blocks per SM, 16 x 16.
  *                  Tiles whose window halo holds more points are split into
  *                  row bands and column ranges, or read from global memory. */
 typedef struct hp_tuning {
@@ -251,6 +254,13 @@ typedef struct hp_tuning {
   int32_t blocks_per_sm;
   int32_t stage_config;
 } hp_tuning;
+
+/* The tile (tile_h x tile_w pixels), staged points per tile and resident
+ * blocks per SM of a stage configuration (0 reads as 1); any output pointer
+ * may be NULL.  HP_ERR_INVALID_ARGUMENT outside 0..5.  No counterpart in the
+ * reference. */
+HP_API int32_t hp_stage_config_info(int32_t config, int32_t* tile_h, int32_t* tile_w, int32_t* stage_points,
+                                    int32_t* blocks_per_sm);
 
 /* hp_quick_sampling with launch tuning (see hp_tuning; NULL = defaults).
  * No counterpart in the reference. */

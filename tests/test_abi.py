@@ -161,9 +161,23 @@ def test_batch_workspace_and_validation(L):
     assert "view 1" in _err(L) and "kernel_size" in _err(L)
     assert L.hp_quick_sampling_batch(two, None, 0, ctypes.byref(t), ws, 1 << 30, None) == -1
     assert L.hp_quick_sampling_batch(two, None, 2, ctypes.byref(t), ws, b - 1, None) == -2
-    for bad_t in (native.HpTuning(4097), native.HpTuning(0, -1), native.HpTuning(0, 0, 4), native.HpTuning(0, 0, -1)):
+    for bad_t in (native.HpTuning(4097), native.HpTuning(0, -1), native.HpTuning(0, 0, 6), native.HpTuning(0, 0, -1)):
         assert L.hp_quick_sampling_batch(two, None, 2, ctypes.byref(bad_t), ws, b, None) == -1
         assert "tuning" in _err(L)
+
+
+def test_stage_config_info(L):
+    shapes = {c: native.stage_config_info(c) for c in native.STAGE_CONFIGS}
+    assert native.stage_config_info(0) == shapes[1]
+    for c, d in shapes.items():
+        assert d["tile_h"] * d["tile_w"] == 256 and d["stage_points"] > 0 and d["blocks_per_sm"] >= 1
+    assert {(d["tile_h"], d["tile_w"]) for d in shapes.values()} == {(8, 32), (16, 16)}
+    # a larger stage means fewer resident blocks
+    assert shapes[1]["stage_points"] < shapes[2]["stage_points"] < shapes[3]["stage_points"]
+    assert shapes[1]["blocks_per_sm"] > shapes[2]["blocks_per_sm"] > shapes[3]["blocks_per_sm"]
+    for bad in (6, -1):
+        assert L.hp_stage_config_info(bad, None, None, None, None) == -1
+        assert "stage_config" in _err(L)
 
 
 def test_pts2plane_checks_workspace(L):

@@ -104,7 +104,7 @@ def test_tuning_does_not_change_outputs():
     r.run()
     torch.cuda.synchronize()
     first = [tuple(t.clone() for t in r.outputs(i)) for i in range(len(r.views))]
-    cases = [(1, 0, 1), (64, 1, 2), (160, 2, 3), (320, 3, 1), (224, 0, 2), (4096, 0, 3)]
+    cases = [(1, 0, 1), (64, 1, 2), (160, 2, 3), (320, 3, 4), (224, 0, 5), (4096, 0, 4), (1, 0, 5)]
     cases += [(320, 0, c) for c in native.STAGE_CONFIGS]
     for heavy, blocks, stage in cases:
         r.tuning = ops.make_tuning(heavy_window=heavy, blocks_per_sm=blocks, stage_config=stage)
@@ -122,3 +122,20 @@ def test_autotuner_caches_per_shape_class():
     assert tuner.cache[tuner.key(r)] == choice
     assert tuner.tune(r) == choice
     assert (r.tuning.stage_config, r.tuning.heavy_window) == choice
+
+
+def test_view_pipeline_tune_keeps_outputs():
+    """ViewPipeline.tune picks one of the stage configurations and the per-view outputs stay the same."""
+    from hashpoint.engine import CameraTable, ViewPipeline
+    sc = synth.make_sphere(n=30000, width=160, height=120, f=220.0)
+    X = torch.from_numpy(sc.xyz).cuda()
+    cams = CameraTable(sc.cameras, "cuda")
+    s = cams.struct(0)
+    pipe = ViewPipeline(len(sc.xyz), 120, 160, sc.options, "cuda")
+    before = [t.clone() for t in pipe.render(X, s)]
+    cfg = pipe.tune(X, [s], reps=1)
+    assert cfg in native.STAGE_CONFIGS and pipe.tuning.stage_config == cfg
+    after = pipe.render(X, s)
+    torch.cuda.synchronize()
+    for a, b in zip(before, after):
+        assert torch.equal(a.view(torch.uint8), b.view(torch.uint8))

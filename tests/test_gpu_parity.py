@@ -246,6 +246,37 @@ def test_edge_cases():
         assert np.array_equal(mask, r[3]) and np.array_equal(pc_idx, r[1])
 
 
+def test_more_huge_buckets_than_ctas():
+    """170 buckets of 2100+ entries: more than the 148 CTAs that order the buckets above 2048
+    entries, so each CTA takes several from the list the scan writes; both bucket orders, and
+    hp_scatter_hashtable's depth order over the same runs (it finds them by scanning)."""
+    rng = np.random.default_rng(21)
+    W, Hh, f = 20, 10, 40.0
+    cam = synth.look_at_camera((0, 0, 4), (0, 0, 0), W, Hh, f)
+    c2w, K = cam.c2w.astype(np.float64), cam.K.astype(np.float64)
+    pix = rng.choice(W * Hh, size=170, replace=False)
+    pts = []
+    for p in pix:
+        u, v = p % W + 0.25, p // W + 0.25          # inside pixel (p % W, p // W) under floor and round alike
+        d = rng.uniform(2.0, 6.0, size=2100 + int(rng.integers(0, 60)))
+        ray = np.linalg.solve(K, np.array([u, v, 1.0]))
+        cam_pts = d[:, None] * ray[None, :]
+        pts.append(cam_pts @ c2w[:3, :3].T + c2w[:3, 3])
+    xyz = np.concatenate(pts)[rng.permutation(sum(len(q) for q in pts))].astype(np.float32)
+    oc = O.camera_from(cam)
+    for sort in (False, True):
+        sidx, sdep, hsh = (H(t) for t in ops.pts2plane(D(xyz), D(cam.w2c), D(cam.K), Hh, W, sort))
+        oi, od, oh = O.pts2plane(xyz, oc, sort)
+        assert (oh[:, 1] > 2048).sum() == 170
+        assert np.array_equal(hsh, oh) and np.array_equal(sidx, oi) and np.array_equal(bits(sdep), bits(od))
+    # runs already grouped by pixel (the stable order), then depth-sorted inside each run
+    oi, od, oh = O.pts2plane(xyz, oc, False)
+    pid = np.repeat(np.arange(W * Hh, dtype=np.int32), np.maximum(oh[:, 1], 0))
+    s_idx, s_dep, s_h = (H(t) for t in ops.scatter_hashtable(D(oi), D(pid), D(od), Hh, W, True))
+    r_idx, r_dep, r_h = O.scatter_hashtable(oi, pid, od, Hh, W, True)
+    assert np.array_equal(s_h, r_h) and np.array_equal(s_idx, r_idx) and np.array_equal(bits(s_dep), bits(r_dep))
+
+
 def test_repeatable():
     xyz, cam, opt, sort = _case(*CASES["clusters_192x160_k5_S16"])
     a = _run_case(xyz, cam, opt, sort)
