@@ -6,13 +6,15 @@
 // per pixel binary-search the sorted array and copy its run.  Here the pixel
 // ids are a small dense key range, so the sort is a counting sort:
 //
-//   k_project_count   one pass over xyz: pixel id + depth with the reference's
-//                     exact rounding, atomic slot within the pixel's bucket
-//   k_block_sums      per-block totals of the H*W counts
-//   k_scan_hash       exclusive scan -> hash_table (start, count) / (-1, -1)
+//   k_project_count   one pass over xyz, four points per thread: pixel id +
+//                     depth with the reference's exact rounding, atomic slot
+//                     within the pixel's bucket (four atomics in flight)
+//   k_scan_hash       single-pass exclusive scan of the H*W counts (tiles
+//                     add up the totals of the tiles before them) ->
+//                     hash_table (start, count) / (-1, -1)
 //   k_scatter         every point to start + slot of a scratch copy, one
-//                     16-byte (id, depth, pixel) record per entry; -1 into the
-//                     off-image tail of the outputs
+//                     16-byte (id, depth, bucket start, bucket count) record
+//                     per entry; -1 into the off-image tail of the outputs
 //   k_order           one thread per bucket entry: its rank among its bucket's
 //                     entries gives its final position (buckets <= 2048)
 //   k_sort_huge_list  buckets above 2048 entries, which k_scan_hash lists as
@@ -38,6 +40,11 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;                    // counts per thread in the scan
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kHugeThreads = 512;
+// Look-back words of the scan: a status bit above the tile's total in the
+// low 32 bits (0 = not yet published).
+constexpr unsigned long long kAggregate = 1ull << 62;
+constexpr int kLookBackSpins = 1 << 16;  // polls of one predecessor (about 64 ns apart) before giving up
+constexpr int kScanMaxTiles = 256;       // blocks of the scan (each a run of chunks of kScanTile pixels)
 
 // Bucket sort key: the point id (sort == 0) or (depth, id) with depth mapped to
 // an order-preserving integer (-0.0 folded onto +0.0 as float comparison does).
@@ -51,42 +58,69 @@ __device__ __forceinline__ unsigned long long sort_key(int id, float depth, int 
 // ---------------------------------------------------------------------------
 // projection + count (epcq.py:251-274 restated with the GEMMs' rounding)
 // ---------------------------------------------------------------------------
+// One point: (pixel id, slot in its bucket, depth bits), pixel id H*W when off
+// the image.
+__device__ __forceinline__ int3 project_point(const float* w, const float* k, float x, float y, float z, int H, int W,
+                                              int fused_world, int fused_image, int* __restrict__ counts) {
+  float pc[3];
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    const float* a = w + 4 * r;
+    const float g = fused_world ? __fmaf_rn(a[2], z, __fmaf_rn(a[1], y, __fmul_rn(a[0], x)))
+                                : __fadd_rn(__fadd_rn(__fmul_rn(a[0], x), __fmul_rn(a[1], y)), __fmul_rn(a[2], z));
+    pc[r] = __fadd_rn(g, a[3]);
+  }
+  float s[3];
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    const float* a = k + 3 * r;
+    s[r] = fused_image ? __fmaf_rn(a[2], pc[2], __fmaf_rn(a[1], pc[1], __fmul_rn(a[0], pc[0])))
+                       : __fadd_rn(__fadd_rn(__fmul_rn(a[0], pc[0]), __fmul_rn(a[1], pc[1])), __fmul_rn(a[2], pc[2]));
+  }
+  const int ix = __float2int_rz(__fdiv_rn(s[0], s[2]));
+  const int iy = __float2int_rz(__fdiv_rn(s[1], s[2]));
+  const bool inb = 0 <= ix && ix < W && 0 <= iy && iy < H;
+  const int p = inb ? ix + iy * W : H * W;
+  const int slot = inb ? atomicAdd(counts + p, 1) : 0;
+  return make_int3(p, slot, __float_as_int(pc[2]));
+}
+
+// Four consecutive points per thread: xyz as three 16-byte loads when it is
+// 16-byte aligned (the last partial group, and unaligned inputs, point by
+// point), the (pixel, slot) pairs as two 16-byte stores and the depths as one.
 __global__ void __launch_bounds__(256) k_project_count(const float* __restrict__ xyz, int n,
                                                        const float* __restrict__ w2c, const float* __restrict__ K,
                                                        int H, int W, int fused_world, int fused_image,
                                                        int* __restrict__ counts, int2* __restrict__ pid_slot,
-                                                       float* __restrict__ depth_out) {
+                                                       float* __restrict__ depth) {
   float w[12], k[9];
 #pragma unroll
   for (int i = 0; i < 12; i++) w[i] = __ldg(w2c + i);
 #pragma unroll
   for (int i = 0; i < 9; i++) k[i] = __ldg(K + i);
-  const int hw = H * W;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float x = __ldg(xyz + 3 * (size_t)i), y = __ldg(xyz + 3 * (size_t)i + 1),
-                z = __ldg(xyz + 3 * (size_t)i + 2);
-    float pc[3];
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-      const float* a = w + 4 * r;
-      const float g = fused_world ? __fmaf_rn(a[2], z, __fmaf_rn(a[1], y, __fmul_rn(a[0], x)))
-                                  : __fadd_rn(__fadd_rn(__fmul_rn(a[0], x), __fmul_rn(a[1], y)), __fmul_rn(a[2], z));
-      pc[r] = __fadd_rn(g, a[3]);
+  const bool vec = ((uintptr_t)xyz & 15) == 0;
+  const int groups = (n + 3) >> 2;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += gridDim.x * blockDim.x) {
+    const int i0 = g << 2;
+    if (vec && i0 + 3 < n) {
+      const float4* x4 = reinterpret_cast<const float4*>(xyz) + 3 * (size_t)g;
+      const float4 a = __ldg(x4), b = __ldg(x4 + 1), c = __ldg(x4 + 2);
+      const int3 o0 = project_point(w, k, a.x, a.y, a.z, H, W, fused_world, fused_image, counts);
+      const int3 o1 = project_point(w, k, a.w, b.x, b.y, H, W, fused_world, fused_image, counts);
+      const int3 o2 = project_point(w, k, b.z, b.w, c.x, H, W, fused_world, fused_image, counts);
+      const int3 o3 = project_point(w, k, c.y, c.z, c.w, H, W, fused_world, fused_image, counts);
+      int4* ps = reinterpret_cast<int4*>(pid_slot + i0);
+      ps[0] = make_int4(o0.x, o0.y, o1.x, o1.y);
+      ps[1] = make_int4(o2.x, o2.y, o3.x, o3.y);
+      *reinterpret_cast<int4*>(depth + i0) = make_int4(o0.z, o1.z, o2.z, o3.z);
+    } else {
+      for (int i = i0; i < n && i < i0 + 4; i++) {
+        const int3 o = project_point(w, k, __ldg(xyz + 3 * (size_t)i), __ldg(xyz + 3 * (size_t)i + 1),
+                                     __ldg(xyz + 3 * (size_t)i + 2), H, W, fused_world, fused_image, counts);
+        pid_slot[i] = make_int2(o.x, o.y);
+        depth[i] = __int_as_float(o.z);
+      }
     }
-    float s[3];
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-      const float* a = k + 3 * r;
-      s[r] = fused_image ? __fmaf_rn(a[2], pc[2], __fmaf_rn(a[1], pc[1], __fmul_rn(a[0], pc[0])))
-                         : __fadd_rn(__fadd_rn(__fmul_rn(a[0], pc[0]), __fmul_rn(a[1], pc[1])), __fmul_rn(a[2], pc[2]));
-    }
-    const int ix = __float2int_rz(__fdiv_rn(s[0], s[2]));
-    const int iy = __float2int_rz(__fdiv_rn(s[1], s[2]));
-    const bool inb = 0 <= ix && ix < W && 0 <= iy && iy < H;
-    const int p = inb ? ix + iy * W : hw;
-    const int slot = inb ? atomicAdd(counts + p, 1) : 0;
-    pid_slot[i] = make_int2(p, slot);
-    depth_out[i] = pc[2];
   }
 }
 
@@ -106,72 +140,127 @@ __device__ __forceinline__ int block_reduce_sum(int v, int* sh) {
   return v;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_block_sums(const int* __restrict__ counts, int hw,
-                                                             int* __restrict__ block_sums) {
-  __shared__ int sh[32];
-  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-  int s = 0;
-#pragma unroll
-  for (int j = 0; j < kScanItems; j++)
-    if (base + j < hw) s += counts[base + j];
-  s = block_reduce_sum(s, sh);
-  if (threadIdx.x == 0) block_sums[blockIdx.x] = s;
-}
-
-// Exclusive scan of counts -> hash_table; the block's carry-in is the sum of
-// the preceding blocks' totals.
-// Also lists the pixels whose buckets exceed kRankMax (count in scalars[1]),
-// for k_sort_huge_list.
-__global__ void __launch_bounds__(kScanThreads) k_scan_hash(const int* __restrict__ counts, int hw,
-                                                            const int* __restrict__ block_sums,
+// Single-pass exclusive scan of counts -> hash_table.  The image's pixels are
+// cut into chunks of kScanTile; at most kScanMaxTiles blocks ("tiles") each
+// take a contiguous run of chunks, in the order the tiles start (their index
+// comes from a counter), so a tile only ever waits on tiles already running.
+// A tile sums its run and publishes the total; its first warp then adds up
+// the totals of all earlier tiles (a look-back over totals alone: no tile
+// waits on another's running total, so there is no chain), and the tile scans
+// its run chunk by chunk from that carry.  Every poll of an earlier tile is
+// bounded (kLookBackSpins); a tile that gives up counts that tile as empty
+// and sets scalars[3] (the table is then wrong; this does not happen while
+// the tiles it waits on are running).  Also lists the pixels whose
+// buckets exceed kRankMax (count in scalars[1]), for k_sort_huge_list.
+// scalars[2]: the tile counter; scalars[0]: the points inside the image.
+__global__ void __launch_bounds__(kScanThreads) k_scan_hash(const int* __restrict__ counts, int hw, int chunks_per_tile,
+                                                            unsigned long long* __restrict__ look,
                                                             int2* __restrict__ hash, int* __restrict__ scalars,
                                                             int* __restrict__ huge) {
   __shared__ int sh[32];
   __shared__ int warp_tot[32];
-  int carry = 0;
-  for (int b = threadIdx.x; b < blockIdx.x; b += blockDim.x) carry += block_sums[b];
-  carry = block_reduce_sum(carry, sh);
-
-  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-  int c[kScanItems];
-  int local = 0;
-#pragma unroll
-  for (int j = 0; j < kScanItems; j++) {
-    c[j] = base + j < hw ? counts[base + j] : 0;
-    local += c[j];
-  }
-  // block exclusive scan of `local`
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int incl = local;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += t;
-  }
-  if (lane == 31) warp_tot[warp] = incl;
+  __shared__ int s_tile, s_carry;
+  if (threadIdx.x == 0) s_tile = atomicAdd(scalars + 2, 1);
   __syncthreads();
+  const int tile = s_tile;
+  const int nchunks = (hw + kScanTile - 1) / kScanTile;
+  const int ch0 = min(nchunks, tile * chunks_per_tile), ch1 = min(nchunks, ch0 + chunks_per_tile);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  static_assert(kScanItems == 4, "one int4 of counts per thread");
+  // a thread's four counts (an int4: base is a multiple of 4 and counts is 256-byte aligned)
+  auto load4 = [&](int base, int* c) {
+    if (base + 3 < hw) {
+      const int4 v = *reinterpret_cast<const int4*>(counts + base);
+      c[0] = v.x, c[1] = v.y, c[2] = v.z, c[3] = v.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; j++) c[j] = base + j < hw ? counts[base + j] : 0;
+    }
+  };
+  // the run's total
+  int part = 0;
+  for (int ch = ch0; ch < ch1; ch++) {
+    int c[4];
+    load4(ch * kScanTile + threadIdx.x * kScanItems, c);
+    part += c[0] + c[1] + c[2] + c[3];
+  }
+  const int total = block_reduce_sum(part, sh);
   if (warp == 0) {
-    int wt = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
-    int wi = wt;
+    if (lane == 0) atomicExch(look + tile, kAggregate | (unsigned)total);
+    int carry = 0;
+    for (int q = lane; q < tile; q += 32) {
+      unsigned long long f = *(volatile unsigned long long*)(look + q);
+      for (int spin = 0; (f >> 62) == 0; spin++) {
+        if (spin == kLookBackSpins) {
+          atomicExch(scalars + 3, 1);
+          f = kAggregate;  // counted as empty
+          break;
+        }
+        __nanosleep(64);
+        f = *(volatile unsigned long long*)(look + q);
+      }
+      carry += (int)(unsigned)(f & 0xffffffffu);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) carry += __shfl_xor_sync(0xffffffffu, carry, o);
+    if (lane == 0) s_carry = carry;
+  }
+  __syncthreads();
+  int run = s_carry;  // points before the current chunk
+
+  for (int ch = ch0; ch < ch1; ch++) {
+    const int base = ch * kScanTile + threadIdx.x * kScanItems;
+    int c[kScanItems];
+    load4(base, c);
+    const int local = c[0] + c[1] + c[2] + c[3];
+    // block exclusive scan of `local`
+    int incl = local;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, wi, o);
-      if (lane >= o) wi += t;
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
     }
-    warp_tot[lane] = wi - wt;
-  }
-  __syncthreads();
-  int off = carry + warp_tot[warp] + incl - local;
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const int wt = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+      int wi = wt;
 #pragma unroll
-  for (int j = 0; j < kScanItems; j++) {
-    const int p = base + j;
-    if (p < hw) {
-      hash[p] = c[j] > 0 ? make_int2(off, c[j]) : make_int2(-1, -1);
-      if (c[j] > kRankMax) huge[atomicAdd(scalars + 1, 1)] = p;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += t;
+      }
+      warp_tot[lane] = wi - wt;
+      sh[lane] = wi;  // sh[31]: the chunk's total
     }
-    off += c[j];
+    __syncthreads();
+    int off = run + warp_tot[warp] + incl - local;
+    int o[kScanItems];
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+      o[j] = off;
+      if (c[j] > kRankMax && base + j < hw) huge[atomicAdd(scalars + 1, 1)] = base + j;
+      off += c[j];
+    }
+    auto entry = [&](int j) { return c[j] > 0 ? make_int2(o[j], c[j]) : make_int2(-1, -1); };
+    if (base + 3 < hw) {  // 16-byte stores (hash_table is 8-byte aligned: two int4 need 16)
+      const int2 e0 = entry(0), e1 = entry(1), e2 = entry(2), e3 = entry(3);
+      if (((uintptr_t)(hash + base) & 15) == 0) {
+        reinterpret_cast<int4*>(hash + base)[0] = make_int4(e0.x, e0.y, e1.x, e1.y);
+        reinterpret_cast<int4*>(hash + base)[1] = make_int4(e2.x, e2.y, e3.x, e3.y);
+      } else {
+        hash[base] = e0, hash[base + 1] = e1, hash[base + 2] = e2, hash[base + 3] = e3;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < kScanItems; j++)
+        if (base + j < hw) hash[base + j] = entry(j);
+    }
+    run += sh[31];
+    __syncthreads();  // warp_tot and sh are rewritten by the next chunk
   }
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) scalars[0] = off;  // points inside the image
+  if (ch1 == nchunks && ch0 < ch1 && threadIdx.x == 0) scalars[0] = run;  // points inside the image
 }
 
 // ---------------------------------------------------------------------------
@@ -184,7 +273,10 @@ __global__ void __launch_bounds__(256) k_scatter(int n, int hw, const int2* __re
   const int n_in = scalars[0];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int2 ps = pid_slot[i];
-    if (ps.x < hw) tmp[hash[ps.x].x + ps.y] = make_int4(i, __float_as_int(depth[i]), ps.x, 0);
+    if (ps.x < hw) {
+      const int2 h = hash[ps.x];
+      tmp[h.x + ps.y] = make_int4(i, __float_as_int(depth[i]), h.x, h.y);
+    }
     if (i >= n_in) {
       out_idx[i] = -1;
       out_depth[i] = -1.0f;
@@ -207,47 +299,67 @@ __device__ __forceinline__ unsigned long long entry_key(const BucketOrder& bo, i
   return sort_key(bo.by_position ? pos : id, depth, bo.by_depth);
 }
 
-// Bucket entries in position order: hp_pts2plane's packed scratch records ...
+// Bucket entries in position order: hp_pts2plane's packed scratch records,
+// which carry their bucket ...
 struct PackedEntries {
-  const int4* rec;  // (id, depth bits, pixel, 0)
-  __device__ __forceinline__ int pixel(int j) const { return __ldg(&rec[j].z); }
+  const int4* rec;  // (id, depth bits, bucket start, bucket count)
+  // entry j: its bucket (start, count) and (id, depth bits); false if none
+  __device__ __forceinline__ bool entry(int j, const int2*, int, int2& bucket, int2& e) const {
+    const int4 r = __ldg(rec + j);
+    bucket = make_int2(r.z, r.w);
+    e = make_int2(r.x, r.y);
+    return true;
+  }
   __device__ __forceinline__ int2 id_depth(int j) const { return __ldg(reinterpret_cast<const int2*>(rec + j)); }
+  __device__ __forceinline__ int id_at(int j) const { return __ldg(reinterpret_cast<const int*>(rec + j)); }
 };
 
-// ... or the caller's sorted arrays (hp_scatter_hashtable).
+// ... or the caller's sorted arrays (hp_scatter_hashtable), whose buckets come
+// from the hash table.
 struct SplitEntries {
   const int* id;
   const float* depth;
   const int* pid;
-  __device__ __forceinline__ int pixel(int j) const { return __ldg(pid + j); }
+  __device__ __forceinline__ bool entry(int j, const int2* hash, int hw, int2& bucket, int2& e) const {
+    const int p = __ldg(pid + j);
+    if (p < 0 || p >= hw) return false;
+    bucket = __ldg(hash + p);
+    e = id_depth(j);
+    return true;
+  }
   __device__ __forceinline__ int2 id_depth(int j) const {
     return make_int2(__ldg(id + j), __float_as_int(__ldg(depth + j)));
   }
+  __device__ __forceinline__ int id_at(int j) const { return __ldg(id + j); }
 };
 
 // One thread per entry j < n_in of the scratch copy: rank among the entries of
 // its bucket -> final position.  Buckets of one entry are copied; buckets above
-// kRankMax are left to k_sort_huge_list / k_sort_huge_scan.
-template <class Entries>
+// kRankMax are left to k_sort_huge_list / k_sort_huge_scan.  The order mode
+// is a template argument so that the rank loop -- the kernel's instructions
+// are mostly its iterations -- compares ids alone when ordering by id.
+template <class Entries, int kByDepth, int kByPosition>
 __global__ void __launch_bounds__(256) k_order(Entries in, const int2* __restrict__ hash, int hw,
                                                const int* __restrict__ scalars, int n_fixed,
-                                               int* __restrict__ out_idx, float* __restrict__ out_depth,
-                                               BucketOrder bo) {
+                                               int* __restrict__ out_idx, float* __restrict__ out_depth) {
+  const BucketOrder bo{kByDepth, kByPosition};
   const int n_in = n_fixed >= 0 ? n_fixed : scalars[0];
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_in; j += gridDim.x * blockDim.x) {
-    const int p = in.pixel(j);
-    if (p < 0 || p >= hw) continue;
-    const int2 h = hash[p];
+    int2 h, e;
+    if (!in.entry(j, hash, hw, h, e)) continue;
     if (h.y > kRankMax) continue;
-    const int2 e = in.id_depth(j);
     const float d = __int_as_float(e.y);
     int pos = h.x;
     if (h.y > 1) {
-      const unsigned long long kj = entry_key(bo, e.x, d, j);
       int rank = 0;
-      for (int q = h.x; q < h.x + h.y; q++) {
-        const int2 eq = in.id_depth(q);
-        rank += entry_key(bo, eq.x, __int_as_float(eq.y), q) < kj;
+      if constexpr (!kByDepth && !kByPosition) {
+        for (int q = h.x; q < h.x + h.y; q++) rank += in.id_at(q) < e.x;
+      } else {
+        const unsigned long long kj = entry_key(bo, e.x, d, j);
+        for (int q = h.x; q < h.x + h.y; q++) {
+          const int2 eq = in.id_depth(q);
+          rank += entry_key(bo, eq.x, __int_as_float(eq.y), q) < kj;
+        }
       }
       pos += rank;
     }
@@ -373,18 +485,19 @@ __global__ void __launch_bounds__(256) k_runs(const int* __restrict__ point_idx,
 // ---------------------------------------------------------------------------
 static constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Scratch of hp_pts2plane.  The look-back words and the scalars are adjacent,
+// so one memset clears both.
 struct BuildLayout {
-  size_t counts, block_sums, pid_slot, depth, tmp, huge, scalars, total;
+  size_t counts, pid_slot, depth, tmp, huge, look, scalars, total;
 };
 
-static BuildLayout build_layout(int64_t n, int64_t hw) {
-  BuildLayout L;
-  const int64_t nblk = (hw + kScanTile - 1) / kScanTile;
+static constexpr BuildLayout build_layout(int64_t n, int64_t hw) {
+  const int64_t nchunks = (hw + kScanTile - 1) / kScanTile;
+  const int64_t tiles = nchunks < kScanMaxTiles ? nchunks : kScanMaxTiles;
+  BuildLayout L{};
   size_t o = 0;
   L.counts = o;
   o += align256(sizeof(int) * (size_t)(hw > 0 ? hw : 1));
-  L.block_sums = o;
-  o += align256(sizeof(int) * (size_t)(nblk > 0 ? nblk : 1));
   L.pid_slot = o;
   o += align256(sizeof(int2) * (size_t)(n > 0 ? n : 1));
   L.depth = o;
@@ -393,6 +506,9 @@ static BuildLayout build_layout(int64_t n, int64_t hw) {
   o += align256(sizeof(int4) * (size_t)(n > 0 ? n : 1));
   L.huge = o;  // pixels of buckets above kRankMax entries: at most n / (kRankMax + 1)
   o += align256(sizeof(int) * (size_t)(n / (kRankMax + 1) + 1));
+  L.look = o;
+  o += sizeof(unsigned long long) * (size_t)(tiles > 0 ? tiles : 1);
+  o = align256(o);
   L.scalars = o;
   o += 256;
   L.total = o;
@@ -414,7 +530,13 @@ template <class Entries>
 static int32_t launch_order(int hw, int n_fixed, int n_grid, Entries in, const int2* hash, const int* scalars,
                             const int* huge, int* out_idx, float* out_depth, BucketOrder bo, cudaStream_t st) {
   if (n_grid > 0) {
-    k_order<<<grid_for(n_grid, 256), 256, 0, st>>>(in, hash, hw, scalars, n_fixed, out_idx, out_depth, bo);
+    const int g = grid_for(n_grid, 256);
+    if (!bo.by_depth && !bo.by_position)
+      k_order<Entries, 0, 0><<<g, 256, 0, st>>>(in, hash, hw, scalars, n_fixed, out_idx, out_depth);
+    else if (!bo.by_position)
+      k_order<Entries, 1, 0><<<g, 256, 0, st>>>(in, hash, hw, scalars, n_fixed, out_idx, out_depth);
+    else
+      k_order<Entries, 1, 1><<<g, 256, 0, st>>>(in, hash, hw, scalars, n_fixed, out_idx, out_depth);
     if (int32_t rc = check_launch("k_order")) return rc;
   }
   if (huge) {
@@ -465,11 +587,11 @@ extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_cam
   cudaStream_t st = (cudaStream_t)stream;
   char* ws = (char*)workspace;
   int* counts = (int*)(ws + L.counts);
-  int* block_sums = (int*)(ws + L.block_sums);
   int2* pid_slot = (int2*)(ws + L.pid_slot);
   float* depth = (float*)(ws + L.depth);
   int4* tmp = (int4*)(ws + L.tmp);
   int* huge = (int*)(ws + L.huge);
+  unsigned long long* look = (unsigned long long*)(ws + L.look);
   int* scalars = (int*)(ws + L.scalars);
   int2* hash = (int2*)hash_table;
   const int n = (int)n_points;
@@ -477,21 +599,21 @@ extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_cam
   hp_projection_rounding(n_points, &fw, &fi);
 
   if (cudaMemsetAsync(counts, 0, sizeof(int) * hw, st) != cudaSuccess ||
-      cudaMemsetAsync(scalars, 0, 256, st) != cudaSuccess)
+      cudaMemsetAsync(look, 0, L.total - L.look, st) != cudaSuccess)
     return set_error(HP_ERR_CUDA, "hp_pts2plane: cudaMemsetAsync failed: %s", cudaGetErrorString(cudaGetLastError()));
   if (n > 0) {
-    k_project_count<<<grid_for(n, 256), 256, 0, st>>>(xyz, n, cam->w2c, cam->K, H, W, fw, fi, counts, pid_slot,
-                                                      depth);
+    k_project_count<<<grid_for((n + 3) / 4, 256), 256, 0, st>>>(xyz, n, cam->w2c, cam->K, H, W, fw, fi, counts,
+                                                                pid_slot, depth);
     if (int32_t rc = check_launch("k_project_count")) return rc;
   }
-  const int nblk = (int)((hw + kScanTile - 1) / kScanTile);
-  k_block_sums<<<nblk, kScanThreads, 0, st>>>(counts, (int)hw, block_sums);
-  if (int32_t rc = check_launch("k_block_sums")) return rc;
-  k_scan_hash<<<nblk, kScanThreads, 0, st>>>(counts, (int)hw, block_sums, hash, scalars, huge);
+  const int nchunks = (int)((hw + kScanTile - 1) / kScanTile);
+  const int per_tile = (nchunks + kScanMaxTiles - 1) / kScanMaxTiles;
+  const int tiles = (nchunks + per_tile - 1) / per_tile;
+  k_scan_hash<<<tiles, kScanThreads, 0, st>>>(counts, (int)hw, per_tile, look, hash, scalars, huge);
   if (int32_t rc = check_launch("k_scan_hash")) return rc;
   if (n > 0) {
-    k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, (int)hw, pid_slot, depth, hash, scalars, tmp, sorted_point_idx,
-                                                sorted_depth);
+    k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, (int)hw, pid_slot, depth, hash, scalars, tmp,
+                                                sorted_point_idx, sorted_depth);
     if (int32_t rc = check_launch("k_scatter")) return rc;
   }
   return launch_order((int)hw, -1, n, PackedEntries{tmp}, hash, scalars, huge, sorted_point_idx, sorted_depth,
@@ -536,11 +658,8 @@ extern "C" int32_t hp_scatter_hashtable(const int32_t* point_idx, const int32_t*
 namespace hp {
 constexpr int64_t kNoAllocMaxPoints = HP_NOALLOC_MAX_POINTS;
 constexpr int64_t kNoAllocMaxPixels = HP_NOALLOC_MAX_PIXELS;
-constexpr size_t kNoAllocScratchBytes =
-    align256(sizeof(int) * kNoAllocMaxPixels) +
-    align256(sizeof(int) * ((kNoAllocMaxPixels + kScanTile - 1) / kScanTile)) +
-    align256(sizeof(int2) * kNoAllocMaxPoints) + align256(sizeof(float) * kNoAllocMaxPoints) +
-    align256(sizeof(int4) * kNoAllocMaxPoints) + align256(sizeof(int) * (kNoAllocMaxPoints / (kRankMax + 1) + 1)) + 256;
+// build_layout grows with both sizes, so the largest accepted problem bounds every call's scratch
+constexpr size_t kNoAllocScratchBytes = build_layout(kNoAllocMaxPoints, kNoAllocMaxPixels).total;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 // Device address of g_noalloc_scratch per device.  It is looked up again on

@@ -1090,6 +1090,13 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     return sum;
   };
+  // The tile's items are collected in shared memory first and then given
+  // queue positions with one atomic per tile: a chain of returning atomics on
+  // the shared item counter, one per item, made tiles that split into many
+  // items wait on it item by item.  One tile per warp, eight warps per block.
+  __shared__ int3 s_item[8][kTileH * 4];  // (cost, item code, columns)
+  const int wp = threadIdx.x >> 5;
+  int n_it = 0;  // warp-uniform
   // split the tile's rows until each item's halo holds at most `cap` points
   // (the stage's capacity, so no item runs much longer than the average) or
   // is one row
@@ -1107,13 +1114,9 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
         const int c = (int)(((long long)min(hs, 1 << 24) * rows * kTileH * (c1 - c0)) /
                             ((long long)(rows + k - 1) * (c1 - c0 + k - 1)));
         const int w = hs > cap ? c * 4 : c;
-        const int i = atomicAdd(sc.n_items, 1);
-        sc.work[i] = w;
-        sc.item[i] = item_code(t, vb - v0, rows);
-        sc.cols[i] = (c0 << 8) | c1;
-        if (sc.view) sc.view[i] = view;
-        atomicAdd(sc.counts + (sc.view ? view * 32 : 0) + cost_class(w), 1);
+        s_item[wp][n_it] = make_int3(w, item_code(t, vb - v0, rows), (c0 << 8) | c1);
       }
+      n_it++;
     };
     if (sum <= cap) {
       emit(sum, 0, kTileW);
@@ -1129,6 +1132,19 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
       }
     }
     vb += rows;
+  }
+  __syncwarp();
+  int first = 0;
+  if (lane == 0) first = atomicAdd(sc.n_items, n_it);
+  first = __shfl_sync(0xffffffffu, first, 0);
+  for (int j = lane; j < n_it; j += 32) {
+    const int3 e = s_item[wp][j];
+    const int i = first + j;
+    sc.work[i] = e.x;
+    sc.item[i] = e.y;
+    sc.cols[i] = e.z;
+    if (sc.view) sc.view[i] = view;
+    atomicAdd(sc.counts + (sc.view ? view * 32 : 0) + cost_class(e.x), 1);  // result unused: a reduction
   }
 }
 
