@@ -165,17 +165,30 @@ struct SrcGlobal {
 // its id), or id -1 when the id is outside [0, n_points).  Every later fetch
 // of candidate j -- staging or global -- is then one 16-byte load instead of
 // an id load and a dependent point gather.
-__global__ void k_pack_points(const int* __restrict__ sidx, int n_sorted, const float* __restrict__ xyz, int n_points,
-                              float4* __restrict__ pts) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n_sorted) return;
+__device__ __forceinline__ float4 packed_point(const int* __restrict__ sidx, int j, const float* __restrict__ xyz,
+                                               int n_points) {
   const int id = __ldg(sidx + j);
   float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
   if ((unsigned)id < (unsigned)n_points) {
     const float4 q = load_point(xyz, id);
     p = make_float4(q.x, q.y, q.z, __int_as_float(id));
   }
-  pts[j] = p;
+  return p;
+}
+
+// Candidates [j0, j1) packed by one warp, four per lane in flight.
+__device__ __forceinline__ void pack_range(const int* __restrict__ sidx, int j0, int j1, const float* __restrict__ xyz,
+                                           int n_points, float4* __restrict__ pts) {
+  const int lane = threadIdx.x & 31;
+  for (int j = j0 + lane; j < j1; j += 128) {
+    float4 p[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (j + 32 * q < j1) p[q] = packed_point(sidx, j + 32 * q, xyz, n_points);
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (j + 32 * q < j1) pts[j + 32 * q] = p[q];
+  }
 }
 
 // Visit a ray's window candidates in the reference's order -- window rows
@@ -1057,21 +1070,25 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
   const int koff = (k + 1) >> 1, lo = koff - 1, hi = k - koff;
   const int hv0 = max(0, v0 - lo), hv1 = min(H - 1, v_end - 1 + hi);
   const int hu0 = max(0, u0 - lo), hu1 = min(W - 1, u0 + kTileW - 1 + hi);
+  // a second halo column per lane only where the halo is wider than a warp
+  constexpr bool kTwoCols = kTileW + kMaxKernel - 1 > 32;
   const int ua = hu0 + lane, ub = hu0 + 32 + lane;  // this lane's halo columns
-  int ca[kHaloRows], cb[kHaloRows];
+  int ca[kHaloRows], cb[kTwoCols ? kHaloRows : 1];
 #pragma unroll
   for (int h = 0; h < kHaloRows; h++) {
     ca[h] = 0;
-    cb[h] = 0;
+    if constexpr (kTwoCols) cb[h] = 0;
     const int vv = hv0 + h;
     if (vv <= hv1) {
       if (ua <= hu1) {
         const int2 rg = bucket_range(__ldg(hash + (size_t)vv * W + ua), n_sorted);
         ca[h] = min(rg.y - rg.x, cap + 1);
       }
-      if (ub <= hu1) {
-        const int2 rg = bucket_range(__ldg(hash + (size_t)vv * W + ub), n_sorted);
-        cb[h] = min(rg.y - rg.x, cap + 1);
+      if constexpr (kTwoCols) {
+        if (ub <= hu1) {
+          const int2 rg = bucket_range(__ldg(hash + (size_t)vv * W + ub), n_sorted);
+          cb[h] = min(rg.y - rg.x, cap + 1);
+        }
       }
     }
   }
@@ -1079,12 +1096,15 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
   auto halo = [&](int vb, int rows, int c0, int c1) {
     const int r0 = max(0, vb - lo), r1 = min(H - 1, vb + rows - 1 + hi);
     const int x0 = max(0, u0 + c0 - lo), x1 = min(W - 1, u0 + c1 - 1 + hi);
-    const bool ia = ua >= x0 && ua <= x1, ib = ub >= x0 && ub <= x1;
+    const bool ia = ua >= x0 && ua <= x1, ib = kTwoCols && ub >= x0 && ub <= x1;
     int sum = 0;
 #pragma unroll
     for (int h = 0; h < kHaloRows; h++) {
       const int vv = hv0 + h;
-      if (vv >= r0 && vv <= r1) sum += (ia ? ca[h] : 0) + (ib ? cb[h] : 0);
+      if (vv >= r0 && vv <= r1) {
+        sum += ia ? ca[h] : 0;
+        if constexpr (kTwoCols) sum += ib ? cb[h] : 0;
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -1148,12 +1168,21 @@ __device__ __forceinline__ void tile_work(const int2* __restrict__ hash, int n_s
   }
 }
 
+// One warp per tile: its work items, then its share of the candidate packing
+// (packing needs no result of the tile pass, so its loads overlap the tile
+// pass's latency instead of taking a launch of their own).  Three blocks per
+// SM, so one view's tiles (2500 warps at 800 x 800) run in one wave.
 template <int kTileH, int kTileW>
-__global__ void __launch_bounds__(256) k_tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k,
-                                                   int tiles_x, int ntiles, int cap, Sched sc) {
+__global__ void __launch_bounds__(256, 3) k_tile_work(const int2* __restrict__ hash, int n_sorted, int H, int W, int k,
+                                                   int tiles_x, int ntiles, int cap, Sched sc,
+                                                   const int* __restrict__ sidx, const float* __restrict__ xyz,
+                                                   int n_points, float4* __restrict__ pts) {
   const int t = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (t >= ntiles) return;
   tile_work<kTileH, kTileW>(hash, n_sorted, H, W, k, tiles_x, t, 0, cap, sc);
+  const int per = (n_sorted + ntiles - 1) / ntiles;
+  const int j0 = min(n_sorted, t * per);
+  pack_range(sidx, j0, min(n_sorted, j0 + per), xyz, n_points, pts);
 }
 
 __global__ void __launch_bounds__(256) k_tile_order(Sched sc) {
@@ -1456,7 +1485,7 @@ __global__ void k_batch_setup(const hp_view* __restrict__ views, int n_views, in
   }
 }
 
-// Pack every view's candidates (see k_pack_points); slot g of the batch.
+// Pack every view's candidates (see packed_point); slot g of the batch.
 __global__ void k_batch_pack(const SampleArgs* __restrict__ args, const int* __restrict__ pack_base, int n_views,
                              int total) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1472,18 +1501,12 @@ __global__ void k_batch_pack(const SampleArgs* __restrict__ args, const int* __r
   const SampleArgs& a = args[lo];
   const int j = g - pack_base[lo];
   if (j >= a.n_sorted) return;
-  const int id = __ldg(a.sidx + j);
-  float4 p = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-  if ((unsigned)id < (unsigned)a.n_points) {
-    const float4 q = load_point(a.xyz, id);
-    p = make_float4(q.x, q.y, q.z, __int_as_float(id));
-  }
-  const_cast<float4*>(a.pts)[j] = p;
+  const_cast<float4*>(a.pts)[j] = packed_point(a.sidx, j, a.xyz, a.n_points);
 }
 
 // One warp per global tile: find its view, then queue the tile's items.
 template <int kTileH, int kTileW>
-__global__ void __launch_bounds__(256) k_batch_tile_work(const SampleArgs* __restrict__ args,
+__global__ void __launch_bounds__(256, 3) k_batch_tile_work(const SampleArgs* __restrict__ args,
                                                          const int* __restrict__ tile_base, int n_views,
                                                          int total_tiles, int cap, Sched sc) {
   const int g = blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -1542,7 +1565,7 @@ __global__ void k_ray_directions(DevCamera cam, float* __restrict__ dirs) {
 struct SamplingKernels {
   void (*view)(SampleArgs, Sched, int);
   void (*batch)(const SampleArgs*, Sched);
-  void (*tile_work)(const int2*, int, int, int, int, int, int, int, Sched);
+  void (*tile_work)(const int2*, int, int, int, int, int, int, int, Sched, const int*, const float*, int, float4*);
   void (*batch_tile_work)(const SampleArgs*, const int*, int, int, int, Sched);
   size_t smem;
   int cap, blocks, tile_h, tile_w, items_per_tile;
@@ -1813,13 +1836,9 @@ extern "C" int32_t hp_quick_sampling_tuned(const float* xyz, int64_t n_points, c
   cudaStream_t st = (cudaStream_t)stream;
   if (cudaMemsetAsync(sc.counts, 0, 512, st) != cudaSuccess)
     return set_error(HP_ERR_CUDA, "hp_quick_sampling: cudaMemsetAsync failed");
-  if (n_sorted > 0) {
-    k_pack_points<<<(unsigned)((n_sorted + 255) / 256), 256, 0, st>>>(sorted_point_idx, (int)n_sorted, xyz,
-                                                                      (int)n_points, (float4*)(ws + L.pts));
-    if (int32_t rc = check_launch("k_pack_points")) return rc;
-  }
   K.tile_work<<<(ntiles + 7) / 8, 256, 0, st>>>(a.hash, a.n_sorted, cam->height, cam->width, opt->kernel_size, tiles_x,
-                                                 ntiles, K.cap, sc);
+                                                 ntiles, K.cap, sc, sorted_point_idx, xyz, (int)n_points,
+                                                 (float4*)(ws + L.pts));
   if (int32_t rc = check_launch("k_tile_work")) return rc;
   k_tile_order<<<(ntiles + 255) / 256 < 148 ? (ntiles + 255) / 256 : 148, 256, 0, st>>>(sc);
   if (int32_t rc = check_launch("k_tile_order")) return rc;
