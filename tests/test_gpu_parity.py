@@ -218,7 +218,7 @@ def test_edge_cases():
         oi, od, oh = O.pts2plane(xyz, O.camera_from(cam), sort)
         assert np.array_equal(hsh, oh) and np.array_equal(sidx, oi) and np.array_equal(bits(sdep), bits(od))
         assert hsh[:, 1].max() == 6000
-    # three buckets above 2048 entries (the CTAs of k_sort_huge share their list)
+    # three buckets above 2048 entries (k_sort_huge_list: the CTAs share the scan's list)
     cam3 = synth.look_at_camera((0, 0, 4), (0, 0, 0), 16, 12, 50.0, 50.0, 8.5, 6.5)
     xyz3 = np.concatenate([rng.normal(size=(3000, 3)) * 0.001 + np.array([dx, 0.0, 0.0])
                            for dx in (-0.16, 0.0, 0.16)]).astype(np.float32)
