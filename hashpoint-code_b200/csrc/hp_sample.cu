@@ -51,7 +51,6 @@
 
 namespace hp {
 
-constexpr int kThreads = 256;  // threads of a sampling block = pixels of a tile
 #ifndef HP_BIN_LIST
 #define HP_BIN_LIST 6
 #endif
@@ -81,24 +80,29 @@ struct SampleArgs {
 };
 
 // Stage configurations: kCap staged points per tile, kBlocks resident blocks
-// per SM, and the tile: kTileH rows x kTileW pixels (kThreads in all).
-// Shared memory per SM bounds stage and blocks together (and registers per
-// thread follow from the blocks: 64 at 4 blocks, 80 at 3, 128 at 2).  A larger
-// stage splits fewer dense tiles into row bands (less re-staging of shared
-// halo rows) but keeps fewer warps resident; a square tile stages a smaller
-// window halo per ray (20 x 20 cells for 256 rays against 12 x 36 at k = 5).
-// Which wins depends on how the cloud's points spread over the image, so the
-// launch picks one (hp_tuning.stage_config) and hashpoint.batch.Autotuner
-// searches them.
+// per SM, and the tile: kTileH rows x kTileW pixels, one thread per pixel
+// (kThreads = 256 or 128 threads per block).  Shared memory per SM bounds
+// stage and blocks together, and registers per thread follow from the
+// resident threads: 64 at 4 x 256 or 8 x 128, 80 at 3 x 256 or 6 x 128, 128 at
+// 2 x 256.  A larger stage splits fewer dense tiles into row bands (less
+// re-staging of shared halo rows) but keeps fewer warps resident; a square
+// tile stages a smaller window halo per ray (20 x 20 cells for 256 rays
+// against 12 x 36 at k = 5).  Which wins depends on how the cloud's points
+// spread over the image, so the launch picks one (hp_tuning.stage_config) and
+// hashpoint.batch.Autotuner searches them.  (128-thread blocks on 8 x 16 tiles
+// -- 4 warps waiting at a tile's end instead of 8, for a 12 x 20 halo per 128
+// rays -- measured 3-5% slower on the shapes views and 12-17% on the clustered
+// ones, with 1216 points x 8 blocks and 1856 x 6, so none is offered.)
 template <int kCap_, int kBlocks_, int kTileH_, int kTileW_>
 struct StageCfg {
   static constexpr int kCap = kCap_;
   static constexpr int kBlocks = kBlocks_;
   static constexpr int kTileH = kTileH_;
   static constexpr int kTileW = kTileW_;
+  static constexpr int kThreads = kTileH * kTileW;
   static constexpr int kHaloMax = (kTileH + kMaxKernel - 1) * (kTileW + kMaxKernel - 1);
   static constexpr int kItemsPerTile = kTileH * 4;  // rows, each in up to four column quarters
-  static_assert(kTileH * kTileW == kThreads && kTileW >= 4 && kTileW <= 32 && kTileH <= 16, "tile shape");
+  static_assert((kThreads == 256 || kThreads == 128) && kTileW >= 4 && kTileW <= 32 && kTileH <= 16, "tile shape");
 };
 using Cfg2560x4 = StageCfg<2560, 4, 8, 32>;     // 40 KB stage, 4 blocks per SM, 8 x 32 tiles (the default)
 using Cfg3712x3 = StageCfg<3712, 3, 8, 32>;     // 58 KB stage, 3 blocks per SM
@@ -114,18 +118,18 @@ struct Stage {
   float4 cand[Cfg::kCap];   // x, y, z, id (as int bits; -1 = invalid id)
   int cls[kClasses];        // rays per window-size class
   int cls_base[kClasses];   // first rank of each class
-  int order[kThreads];      // pixel of each rank, heaviest class first
+  int order[Cfg::kThreads];  // pixel of each rank, heaviest class first
   int off[Cfg::kHaloMax + 1];  // staged offset of each halo cell, exclusive prefix
   int start[Cfg::kHaloMax];    // the cell's first index in sorted_point_idx
-  int warp_tot[kThreads / 32];
+  int warp_tot[Cfg::kThreads / 32];
   int next_unit;            // next work unit of the tile (see process_tile)
-  unsigned kept[kMaskWords][kThreads];  // per thread: window positions pass A accepted
+  unsigned kept[kMaskWords][Cfg::kThreads];  // per thread: window positions pass A accepted
 };
 // kBlocks CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
 template <class Cfg>
 constexpr bool fits_sm() {
   return Cfg::kBlocks * (sizeof(Stage<Cfg>) + 16 + 1024) <= 228 * 1024 && Cfg::kItemsPerTile <= kMaxItemsPerTile &&
-         Cfg::kHaloMax <= kCellsPerThread * kThreads;
+         Cfg::kHaloMax <= kCellsPerThread * Cfg::kThreads;
 }
 static_assert(fits_sm<Cfg2560x4>() && fits_sm<Cfg3712x3>() && fits_sm<Cfg5888x2>() && fits_sm<Cfg2560x4Sq>() &&
                   fits_sm<Cfg3712x3Sq>(),
@@ -141,6 +145,7 @@ __device__ __forceinline__ int2 bucket_range(int2 h, int n_sorted) {
 template <class Cfg>
 struct SrcStaged {
   static constexpr bool kStaged = true;
+  static constexpr int kKeptStride = Cfg::kThreads;  // the kept masks' word stride (one column per thread)
   const Stage<Cfg>* st;
   int rv0, ru0, nu;
   __device__ __forceinline__ int cell(int vv, int uu) const { return (vv - rv0) * nu + (uu - ru0); }
@@ -154,6 +159,7 @@ struct SrcStaged {
 // Candidates straight from global memory (tiles whose halo overflows the stage).
 struct SrcGlobal {
   static constexpr bool kStaged = false;
+  static constexpr int kKeptStride = 1;  // no kept masks
   __device__ __forceinline__ int cell(int, int) const { return 0; }
   __device__ __forceinline__ int2 range(const SampleArgs& a, int vv, int uu) const {
     return bucket_range(__ldg(a.hash + (size_t)vv * a.cam.width + uu), a.n_sorted);
@@ -275,7 +281,7 @@ __device__ __forceinline__ void walk_rows(const SampleArgs& a, const Src& src, i
 }
 
 // Visit the candidates whose window positions are set in a kept mask (nw
-// words, stride kThreads), in order; the position is mapped back to the stage
+// words, stride Src::kKeptStride), in order; the position is mapped back to the stage
 // row by row.
 template <class Src, class Body>
 __device__ __forceinline__ void walk_kept(const SampleArgs& a, const Src& src, int v, int u, const unsigned* mask,
@@ -285,7 +291,7 @@ __device__ __forceinline__ void walk_kept(const SampleArgs& a, const Src& src, i
   const int* off = src.st->off;
   int r = -1, rf0 = 0, rf1 = 0, jb = 0;
   for (int w = 0; w < nw; w++) {
-    unsigned m = mask[w * kThreads];
+    unsigned m = mask[w * Src::kKeptStride];
     while (m) {
       const int f = (w << 5) + __ffs(m) - 1;
       m &= m - 1;
@@ -384,7 +390,7 @@ __device__ __forceinline__ float ray_t(const Ray& r, bool unit, float px, float 
 }
 
 // `kept` (staged tiles only; else null) is this thread's kept-candidate mask
-// (kMaskWords words, stride kThreads).  For windows with unclamped columns and
+// (kMaskWords words, stride Src::kKeptStride).  For windows with unclamped columns and
 // at most kMaskWords * 32 candidates, pass A records the positions it keeps
 // there and pass B visits only those, without the radius test or the cap.
 template <class Src>
@@ -411,7 +417,7 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
       }
       if (T <= kMaskWords * 32) {
         masked_T = T;
-        for (int w = 0; w < (T + 31) >> 5; w++) kept[w * kThreads] = 0u;
+        for (int w = 0; w < (T + 31) >> 5; w++) kept[w * Src::kKeptStride] = 0u;
       }
     }
   }
@@ -439,14 +445,14 @@ __device__ __forceinline__ void sample_ray(const SampleArgs& a, const Src& src, 
       walk_rows(a, src, v, u, kKeptPerCell, [&](const float4& p, int f) -> bool {
         if (!keep(p)) return false;
         if ((f >> 5) != wi) {
-          if (word) kept[wi * kThreads] = word;
+          if (word) kept[wi * Src::kKeptStride] = word;
           wi = f >> 5;
           word = 0u;
         }
         word |= 1u << (f & 31);
         return true;
       });
-      if (word) kept[wi * kThreads] = word;
+      if (word) kept[wi * Src::kKeptStride] = word;
     }
   }
   if (!masked) walk_window(a, src, v, u, kKeptPerCell, keep);
@@ -1283,7 +1289,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<Cfg>& st
   for (int q = 0; q < warp; q++) base += st.warp_tot[q];
   int total = 0;
 #pragma unroll
-  for (int q = 0; q < kThreads / 32; q++) total += st.warp_tot[q];
+  for (int q = 0; q < Cfg::kThreads / 32; q++) total += st.warp_tot[q];
 #pragma unroll
   for (int q = 0; q < kCellsPerThread; q++) {
     const int c = tid * kCellsPerThread + q;
@@ -1295,7 +1301,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<Cfg>& st
 
   const bool staged = total <= kCap;
   if (staged) {
-    for (int i = tid; i < total; i += kThreads) {
+    for (int i = tid; i < total; i += Cfg::kThreads) {
       int lo_c = 0, hi_c = ncells;  // off[lo_c] <= i < off[hi_c]
       while (hi_c - lo_c > 1) {
         const int mid = (lo_c + hi_c) >> 1;
@@ -1361,7 +1367,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<Cfg>& st
     __syncthreads();
     st.order[st.cls_base[c] + local] = tid;
     nheavy = st.cls[0];
-    nvalid = kThreads - st.cls[kClasses - 1];
+    nvalid = Cfg::kThreads - st.cls[kClasses - 1];
     __syncthreads();
   }
   const int ngroups = (nvalid - nheavy + 31) >> 5;
@@ -1392,7 +1398,7 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<Cfg>& st
 }
 
 template <class Cfg>
-__global__ void __launch_bounds__(kThreads, Cfg::kBlocks) k_quick_sampling(SampleArgs a, Sched sc, int tiles_x) {
+__global__ void __launch_bounds__(Cfg::kThreads, Cfg::kBlocks) k_quick_sampling(SampleArgs a, Sched sc, int tiles_x) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Stage<Cfg>& st = *reinterpret_cast<Stage<Cfg>*>(smem_raw);
   __shared__ int s_next;
@@ -1528,7 +1534,7 @@ __global__ void __launch_bounds__(256, 3) k_batch_tile_work(const SampleArgs* __
 // The persistent sampling kernel over the batch's queue; each item's view
 // arguments are loaded into shared memory before the tile is processed.
 template <class Cfg>
-__global__ void __launch_bounds__(kThreads, Cfg::kBlocks)
+__global__ void __launch_bounds__(Cfg::kThreads, Cfg::kBlocks)
     k_quick_sampling_batch(const SampleArgs* __restrict__ args, Sched sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Stage<Cfg>& st = *reinterpret_cast<Stage<Cfg>*>(smem_raw);
@@ -1568,7 +1574,7 @@ struct SamplingKernels {
   void (*tile_work)(const int2*, int, int, int, int, int, int, int, Sched, const int*, const float*, int, float4*);
   void (*batch_tile_work)(const SampleArgs*, const int*, int, int, int, Sched);
   size_t smem;
-  int cap, blocks, tile_h, tile_w, items_per_tile;
+  int cap, blocks, threads, tile_h, tile_w, items_per_tile;
 };
 template <class Cfg>
 static SamplingKernels sampling_kernels() {
@@ -1579,14 +1585,15 @@ static SamplingKernels sampling_kernels() {
           sizeof(Stage<Cfg>),
           Cfg::kCap,
           Cfg::kBlocks,
+          Cfg::kThreads,
           Cfg::kTileH,
           Cfg::kTileW,
           Cfg::kItemsPerTile};
 }
 static const SamplingKernels& stage_kernels(int config) {  // config 1..kStageConfigs
-  static const SamplingKernels table[kStageConfigs] = {sampling_kernels<Cfg2560x4>(), sampling_kernels<Cfg3712x3>(),
-                                                       sampling_kernels<Cfg5888x2>(), sampling_kernels<Cfg2560x4Sq>(),
-                                                       sampling_kernels<Cfg3712x3Sq>()};
+  static const SamplingKernels table[kStageConfigs] = {
+      sampling_kernels<Cfg2560x4>(),   sampling_kernels<Cfg3712x3>(), sampling_kernels<Cfg5888x2>(),
+      sampling_kernels<Cfg2560x4Sq>(), sampling_kernels<Cfg3712x3Sq>()};
   return table[config - 1];
 }
 
@@ -1625,7 +1632,7 @@ int32_t sampling_grid(int config, int* blocks, int* sm_count = nullptr) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(K.batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem);
     int sms = 0, per_sm = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, K.view, kThreads, K.smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, K.view, K.threads, K.smem);
     if (e != cudaSuccess) return set_error(HP_ERR_CUDA, "hp_quick_sampling: kernel set-up: %s", cudaGetErrorString(e));
     g = sms * (per_sm > 0 ? per_sm : 1);
     sm_counts[dev] = sms;
@@ -1844,7 +1851,7 @@ extern "C" int32_t hp_quick_sampling_tuned(const float* xyz, int64_t n_points, c
   if (int32_t rc = check_launch("k_tile_order")) return rc;
   // a split tile yields up to items_per_tile items: size the persistent grid by those, not by tiles
   const int64_t max_items = (int64_t)ntiles * K.items_per_tile;
-  K.view<<<blocks < max_items ? blocks : (int)max_items, kThreads, K.smem, st>>>(a, sc, tiles_x);
+  K.view<<<blocks < max_items ? blocks : (int)max_items, K.threads, K.smem, st>>>(a, sc, tiles_x);
   return check_launch("k_quick_sampling");
 }
 
@@ -1957,7 +1964,7 @@ extern "C" int32_t hp_quick_sampling_batch(const hp_view* views, const hp_view* 
   k_batch_order_place<<<(nt + 255) / 256 < 148 ? (nt + 255) / 256 : 148, 256, 0, st>>>(sc, base);
   if (int32_t rc = check_launch("k_batch_order_place")) return rc;
   const int64_t grid_items = (int64_t)nt * K.items_per_tile;
-  K.batch<<<blocks < grid_items ? blocks : (int)grid_items, kThreads, K.smem, st>>>(args, sc);
+  K.batch<<<blocks < grid_items ? blocks : (int)grid_items, K.threads, K.smem, st>>>(args, sc);
   return check_launch("k_quick_sampling_batch");
 }
 
