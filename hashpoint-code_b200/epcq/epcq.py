@@ -36,6 +36,31 @@ def _scalar(v):
     return v.item() if isinstance(v, torch.Tensor) else v
 
 
+def _host_values(*vals):
+    """The values of Python numbers and one-element tensors as Python numbers, the tensors read
+    back with one device-to-host copy per device (the reference's callers pass 0-d CUDA tensors for
+    fx..height, opt/render_image.py:61-68; reading each with .item() waits on the stream once per
+    value).  Tensors holding integers come back as int, the rest as float (float32 values and
+    integers below 2^53 survive the float64 round trip exactly)."""
+    out = list(vals)
+    groups = {}
+    for i, v in enumerate(vals):
+        if isinstance(v, torch.Tensor):
+            if v.numel() != 1:
+                raise RuntimeError("a camera scalar must hold one element, got shape %s" % (tuple(v.shape),))
+            groups.setdefault(v.device, []).append(i)
+    for dev, idx in groups.items():
+        if len(idx) == 1 or dev.type != "cuda":
+            for i in idx:
+                out[i] = vals[i].item()
+            continue
+        host = torch.stack([vals[i].reshape(()).to(torch.float64) for i in idx]).cpu().tolist()
+        for i, h in zip(idx, host):
+            is_int = not (vals[i].dtype.is_floating_point or vals[i].dtype.is_complex)
+            out[i] = int(h) if is_int else h
+    return out
+
+
 @dataclass
 class CameraSpec:
     c2w: torch.Tensor
@@ -48,12 +73,26 @@ class CameraSpec:
     width: int
     height: int
 
+    def _host(self):
+        """(fx, fy, cx, cy, width, height) as Python numbers.  Tensor fields are read back
+        together and the values kept on the camera while its fields are the same objects at the
+        same version (an in-place change bumps a tensor's version), so the calls of one view --
+        pts2plane, then render_image_hashtable_topk -- read them once."""
+        fields = (self.fx, self.fy, self.cx, self.cy, self.width, self.height)
+        versions = tuple(f._version if isinstance(f, torch.Tensor) else None for f in fields)
+        hit = self.__dict__.get("_host_cache")
+        if hit is not None and all(a is b for a, b in zip(hit[0], fields)) and hit[1] == versions:
+            return hit[2]
+        vals = tuple(_host_values(*fields))
+        if any(isinstance(f, torch.Tensor) for f in fields):
+            self.__dict__["_host_cache"] = (fields, versions, vals)
+        return vals
+
     def _to_cpp(self):
         spec = _C.CameraSpec()
         spec.c2w = self.c2w
         spec.w2c = self.w2c
-        spec.fx, spec.fy, spec.cx, spec.cy = self.fx, self.fy, self.cx, self.cy
-        spec.width, spec.height = self.width, self.height
+        spec.fx, spec.fy, spec.cx, spec.cy, spec.width, spec.height = self._host()
         return spec
 
     @staticmethod
@@ -262,7 +301,8 @@ class NeuralPoints(nn.Module):
     def pts2plane(self, cam: CameraSpec, opt: RenderOptions, pc_xyz: torch.Tensor = None, sort: bool = False):
         """Projection + per-pixel hash table (epcq.py:279-295), in one CUDA library call."""
         xyz = (self.xyz_data if pc_xyz is None else pc_xyz).detach()
-        return ops.pts2plane(xyz, cam.w2c, cam.K, _scalar(cam.height), _scalar(cam.width), sort)
+        width, height = cam._host()[4:]
+        return ops.pts2plane(xyz, cam.w2c, cam.K, height, width, sort)
 
     def render_image_hashtable_topk(self, cam: CameraSpec, opt: RenderOptions,
                                     sorted_point_idx_list: torch.Tensor,
@@ -293,8 +333,8 @@ class FeatureQuery(nn.Module):
     def generate_rays(self, cam: CameraSpec):
         """(rays_o, rays_d) [H, W, 3] through pixel corners, as the reference builds them (epcq.py:333-341)."""
         dev = cam.c2w.device
-        fx, fy, cx, cy = (float(_scalar(v)) for v in (cam.fx, cam.fy, cam.cx, cam.cy))
-        W, H = int(_scalar(cam.width)), int(_scalar(cam.height))
+        fx, fy, cx, cy, W, H = cam._host()
+        fx, fy, cx, cy, W, H = float(fx), float(fy), float(cx), float(cy), int(W), int(H)
         y, x = torch.meshgrid(torch.arange(H, dtype=torch.float32, device=dev),
                               torch.arange(W, dtype=torch.float32, device=dev), indexing="ij")
         d = torch.stack([(x - cx) / fx, (y - cy) / fy, torch.ones_like(x)], dim=-1)
@@ -308,11 +348,11 @@ class FeatureQuery(nn.Module):
         uv = ray_index_uv if ray_index_uv is not None and len(ray_index_uv) != 0 else None
         pc_idx = output_pc_idx if output_pc_idx.dtype == torch.int32 else output_pc_idx.to(torch.int32)
         feat = neuralpoints.feat_data.detach()
+        fx, fy, cx, cy, width = cam._host()[:5]
         return ops.feature_query(neuralpoints.xyz_data.detach().contiguous(), neuralpoints.rgb_data.detach().contiguous(),
                                  neuralpoints.dir_data.detach().contiguous(), feat.contiguous(),
                                  output_sp_xyz.contiguous(), pc_idx.contiguous(), mask_out, cam.c2w,
-                                 _scalar(cam.fx), _scalar(cam.fy), _scalar(cam.cx), _scalar(cam.cy),
-                                 _scalar(cam.width), uv)
+                                 fx, fy, cx, cy, width, uv)
 
 
 def positional_encoding(positions, freqs, ori=False):

@@ -37,6 +37,46 @@ def test_spec_fields_accept_zero_dim_tensors():
         c.c2w = [1, 2]
 
 
+def test_camera_scalars_read_back_together():
+    """CameraSpec._to_cpp takes Python numbers or one-element tensors (the reference's renderer
+    passes 0-d tensors from K and the image size); the values, and int for integer tensors,
+    survive the shared read-back."""
+    K = torch.tensor([[1111.5, 0, 400.25], [0, 1110.75, 399.5], [0, 0, 1]], dtype=torch.float32)
+    fx, fy, cx, cy = E.CameraSpec.decomposeK(K)
+    hw = torch.tensor([800, 640])
+    cam = E.CameraSpec(c2w=torch.eye(4), w2c=torch.eye(4), K=K, fx=fx, fy=fy, cx=cx, cy=cy, height=hw[0],
+                       width=hw[1])
+    spec = cam._to_cpp()
+    assert (spec.fx, spec.fy, spec.cx, spec.cy, spec.width, spec.height) == (1111.5, 1110.75, 400.25, 399.5, 640, 800)
+    vals = E._host_values(fx, 3, 2.5, hw[1], torch.tensor(0.1, dtype=torch.float32))
+    assert vals[:4] == [1111.5, 3, 2.5, 640] and isinstance(vals[3], int)
+    assert vals[4] == float(torch.tensor(0.1, dtype=torch.float32))  # the float32 value, exactly
+    with pytest.raises(RuntimeError):
+        E._host_values(torch.zeros(2))
+
+
+def test_camera_scalars_read_once_per_camera(monkeypatch):
+    """A view's calls share one read-back of its camera's tensor scalars; an in-place change of
+    one of them, or a new field object, reads them again."""
+    calls = []
+    real = E._host_values
+    monkeypatch.setattr(E, "_host_values", lambda *v: calls.append(1) or real(*v))
+    K = torch.tensor([[100.0, 0, 32.0], [0, 90.0, 24.0], [0, 0, 1]])
+    fx, fy, cx, cy = E.CameraSpec.decomposeK(K)
+    hw = torch.tensor([48, 64])
+    cam = E.CameraSpec(c2w=torch.eye(4), w2c=torch.eye(4), K=K, fx=fx, fy=fy, cx=cx, cy=cy, height=hw[0],
+                       width=hw[1])
+    assert cam._host() == (100.0, 90.0, 32.0, 24.0, 64, 48)
+    cam._to_cpp()
+    assert len(calls) == 1
+    K[0, 0] = 120.0  # in place: fx's version moves
+    assert cam._host()[0] == 120.0 and len(calls) == 2
+    cam.width = 80  # a new object
+    assert cam._host()[4] == 80 and len(calls) == 3
+    plain = E.CameraSpec(c2w=torch.eye(4), w2c=torch.eye(4), K=K, fx=1.0, fy=2.0, cx=3.0, cy=4.0, width=5, height=6)
+    assert plain._host() == (1.0, 2.0, 3.0, 4.0, 5, 6)
+
+
 def test_options_to_cpp_roundtrip():
     o = E.RenderOptions(kernel_size=3, num_point_cloud_per_sp=8)
     cpp = o._to_cpp()

@@ -277,6 +277,31 @@ def test_more_huge_buckets_than_ctas():
     assert np.array_equal(s_h, r_h) and np.array_equal(s_idx, r_idx) and np.array_equal(bits(s_dep), bits(r_dep))
 
 
+def test_epcq_camera_scalars_on_the_device():
+    """Through the drop-in epcq API, a camera whose fx..cy are 0-d CUDA tensors taken from K and
+    whose size is a CUDA tensor (as the reference's renderer builds it) gives the same outputs, bit
+    for bit, as the same camera with Python numbers."""
+    from epcq import epcq as E
+    rng = np.random.default_rng(31)
+    xyz = synth.shapes_cloud(rng, 20000)
+    cam = synth.orbit_cameras(rng, 1, 4.0, 96, 80, 120.0)[0]
+    K = D(cam.K)
+    model = E.NeuralPoints(pc_type="pc", points=D(xyz))
+    opt = E.RenderOptions(kernel_size=5, radius_threshold=0.05, num_sample_points_per_ray=8, num_point_cloud_per_sp=8)
+    fx, fy, cx, cy = E.CameraSpec.decomposeK(K)
+    hw = torch.tensor([cam.height, cam.width], device="cuda")
+    cams = [E.CameraSpec(c2w=D(cam.c2w), w2c=D(cam.w2c), K=K, fx=cam.fx, fy=cam.fy, cx=cam.cx, cy=cam.cy,
+                         width=cam.width, height=cam.height),
+            E.CameraSpec(c2w=D(cam.c2w), w2c=D(cam.w2c), K=K, fx=fx, fy=fy, cx=cx, cy=cy, height=hw[0], width=hw[1])]
+    outs = []
+    for c in cams:
+        idx, dep, hsh = model.pts2plane(c, opt)
+        outs.append([H(t) for t in (idx, dep, hsh) + tuple(model.render_image_hashtable_topk(c, opt, idx, dep, hsh))])
+    for a, b in zip(*outs):
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+    assert outs[0][-1].any()
+
+
 def test_repeatable():
     xyz, cam, opt, sort = _case(*CASES["clusters_192x160_k5_S16"])
     a = _run_case(xyz, cam, opt, sort)
