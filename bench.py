@@ -6,11 +6,15 @@ never reads), 100 cameras on a radius-4 sphere looking at the origin,
 800x800 pixels, f=1111, radius 0.008, 5x5 window, K=8 samples, 8 points per
 sample, one launch per view.  Seeded synthetic data (seed 0).
 
-One step = all 100 views through the plain per-view launch: hp_pts2plane
-(projection + per-pixel hash table) then hp_quick_sampling (window search,
-primary-surface selection, sample emission, per-sample points), every output
-written to HBM.  With N GPUs (torchrun) every rank renders its own 100 views
-(weak scaling; no collective on the data path).
+One step = all 100 views through per-view launches: for each view
+hp_pts2plane (projection + per-pixel hash table) then hp_quick_sampling
+(window search, primary-surface selection, sample emission, per-sample
+points), every output written to HBM.  The views are spread over three
+streams, each with its own buffers (hashpoint.engine.ViewRing), so one view's
+build and tile scheduling run in the previous view's sampling tail; the line
+also gives the same launches one after another on one stream
+("single_stream").  With N GPUs (torchrun) every rank renders its own 100
+views (weak scaling; no collective on the data path).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -45,6 +49,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "hashpoint-code_b200"))
 
 METRIC = "rays/s search+sample on 1 B200; served p50/p99 ms vs plain per-view launch"
+RING_DEPTH = 3  # streams (and buffer sets) the per-view launches of a step are spread over
 UNIT = "rays/s"
 WORKLOAD = "shapes-1M-800x800-100views"
 
@@ -200,7 +205,7 @@ def run_gpu(args):
     import torch.distributed as dist
 
     from hashpoint import native, synth
-    from hashpoint.engine import CameraTable, ViewPipeline
+    from hashpoint.engine import CameraTable, ViewPipeline, ViewRing
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -221,14 +226,15 @@ def run_gpu(args):
     xyz = torch.from_numpy(sc.xyz).to(dev)
     feat = torch.from_numpy(sc.feat).to(dev)  # resident, never read by the path
     cams = CameraTable(sc.cameras, dev)
-    pipe = ViewPipeline(len(sc.xyz), 800, 800, sc.options, dev)
+    ring = ViewRing(len(sc.xyz), 800, 800, sc.options, dev, depth=RING_DEPTH)
+    pipe = ring.pipes[0]  # the single-stream form, the tuning and the roofline use one pipeline
     stream = torch.cuda.Stream(dev)
     structs = [cams.struct(i) for i in range(cams.n)]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
     # the sampling kernel's stage configuration for this workload (outputs never depend on it)
     with torch.cuda.stream(stream):
-        stage = pipe.tune(xyz, structs[:5], stream)
+        stage = ring.tune(xyz, structs[:5], stream)
 
     # in-image point count per view (for the algorithmic byte count), outside timing
     n_in = []
@@ -242,7 +248,10 @@ def run_gpu(args):
     out_bytes = HW * S * (12 + 4 + 1 + 4 * P)
     samp_bytes = [16 * ni + 8 * HW + out_bytes for ni in n_in]
 
-    def step(ev_samp=None):
+    def step():  # the timed step: per-view launches over the ring's streams
+        ring.render_many(xyz, structs, stream)
+
+    def step_single(ev_samp=None):  # the same launches on one stream, each sampling call timed
         for i, s in enumerate(structs):
             pipe.build(xyz, s, stream)
             if ev_samp is not None:
@@ -255,6 +264,8 @@ def run_gpu(args):
         for _ in range(args.warmup):
             flush.fill_(1)
             step()
+            flush.fill_(1)
+            step_single()
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
@@ -264,26 +275,42 @@ def run_gpu(args):
     if world > 1:
         dist.barrier()
     t_wall0 = time.perf_counter()
-    step_ms, samp_ms = [], []
+    step_ms = []
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
             flush.fill_(1)  # L2 flushed between steps, outside the step events
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
-            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in structs]
             e0.record(stream)
-            step(ev)
+            step()
             e1.record(stream)
             stream.synchronize()
             step_ms.append(e0.elapsed_time(e1))
-            samp_ms.extend(a.elapsed_time(b) for a, b in ev)
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
     t_wall = time.perf_counter() - t_wall0
-    clk = clocks.stop()
-
     value, ms_per_step = shard.job_rays_per_s(HW * len(structs), sum(step_ms) / len(step_ms), dev)
+
+    # the same on one stream: the sequential per-view figure, and each sampling launch's duration
+    single_ms, samp_ms = [], []
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in structs]
+            e0.record(stream)
+            step_single(ev)
+            e1.record(stream)
+            stream.synchronize()
+            single_ms.append(e0.elapsed_time(e1))
+            samp_ms.extend(a.elapsed_time(b) for a, b in ev)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    single_value, single_ms_per_step = shard.job_rays_per_s(HW * len(structs), sum(single_ms) / len(single_ms), dev)
 
     # roofline of the dominant kernel (k_quick_sampling)
     peaks = {}
@@ -313,10 +340,10 @@ def run_gpu(args):
         torch.cuda.empty_cache()
         downstream = run_downstream(args, dev, xyz, feat, sc, pipe, structs, stream, peak, flush)
         others = run_other_workloads(dev, flush, peak)
-        del pipe
+        del pipe, ring
         torch.cuda.empty_cache()
         refgpu = run_reference_gpu(dev, flush, {
-            WORKLOAD.rsplit("-", 1)[0]: ms_per_step / len(structs),
+            WORKLOAD.rsplit("-", 1)[0]: single_ms_per_step / len(structs),
             "sphere-100k-400x400": others["sphere_100k_400x400"]["ms_per_view"],
             "clusters-3M-1600x1200": others["clusters_3M_1600x1200"]["ms_per_view"]})
         torch.cuda.empty_cache()
@@ -329,7 +356,9 @@ def run_gpu(args):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no public dataset)",
         "config": config_dict(args, {"l2": "flushed between steps (256 MiB write)",
-                                     "path": "plain per-view launch, preallocated buffers",
+                                     "path": "per-view launches (hp_pts2plane + hp_quick_sampling for each view) "
+                                             "over %d streams with a buffer set each (hashpoint.engine.ViewRing)"
+                                             % RING_DEPTH,
                                      "sampling_stage_config": stage_desc(stage)}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "k_quick_sampling", "peak_source": peak_src,
@@ -338,7 +367,9 @@ def run_gpu(args):
         "clocks": clk, "e2e": e2e,
         "gpu_launches": ViewPipeline.KERNELS_PER_VIEW * len(structs) * args.steps,
         "wall_s_timed_region": t_wall,
-        "stages_ms_per_view": {"build_plus_sample": ms_per_step / len(structs), "sample": samp_avg_ms},
+        "stages_ms_per_view": {"build_plus_sample": single_ms_per_step / len(structs), "sample": samp_avg_ms},
+        "single_stream": {"value": single_value, "ms_per_step": single_ms_per_step,
+                          "path": "the same per-view launches one after another on one stream"},
     }
     if downstream is not None:
         result["downstream"] = downstream

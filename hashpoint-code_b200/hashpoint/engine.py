@@ -112,7 +112,58 @@ class ViewPipeline:
         self.sample(xyz, cam, stream)
         return self.sp_xyz, self.pc_idx, self.sp_t, self.mask
 
-    # kernels each render() launches (hp_pts2plane: project/count, block sums,
-    # scan, scatter, order, huge-bucket sort; hp_quick_sampling: tile work,
-    # tile order, sampling)
-    KERNELS_PER_VIEW = 9
+    # kernels each render() launches (hp_pts2plane: project/count, scan,
+    # scatter, order, huge-bucket sort; hp_quick_sampling: tile work with the
+    # packing, tile order, sampling)
+    KERNELS_PER_VIEW = 8
+
+
+class ViewRing:
+    """Many views of one shape through per-view launches, pipelined over `depth` streams.
+
+    View i runs on pipeline i % depth (its own buffers) and that pipeline's stream, so view i+1's
+    hash-table build and tile scheduling run while view i's persistent sampling kernel drains its
+    last work items, and its sampling kernel's blocks start as view i's retire.  Every view is
+    still hp_pts2plane + hp_quick_sampling, each with the outputs the plain launch gives.  A
+    view's outputs stay in its pipeline's buffers until view i + depth reuses them on the same
+    stream: `on_view(i, pipe, stream)` is called right after view i is enqueued, so work it
+    enqueues on `stream` reads them before they are overwritten."""
+
+    def __init__(self, n_points, height, width, options, device, depth=3, sort=False, tuning=None):
+        self.device = torch.device(device)
+        self.pipes = [ViewPipeline(n_points, height, width, options, device, sort, tuning) for _ in range(depth)]
+        self.streams = [torch.cuda.Stream(self.device) for _ in range(depth)]
+
+    @property
+    def depth(self):
+        return len(self.pipes)
+
+    def set_tuning(self, tuning):
+        for p in self.pipes:
+            p.tuning = tuning
+
+    def tune(self, xyz, cams, stream=None, reps=2):
+        """ViewPipeline.tune on the first pipeline; every pipeline then uses its choice."""
+        cfg = self.pipes[0].tune(xyz, cams, stream, reps)
+        self.set_tuning(self.pipes[0].tuning)
+        return cfg
+
+    def render_many(self, xyz, cams, stream=None, on_view=None):
+        """Render `cams` (HpCamera structs); the views' work starts after, and `stream` waits for,
+        everything enqueued on `stream` before the call."""
+        main = stream or torch.cuda.current_stream(self.device)
+        start = torch.cuda.Event()
+        start.record(main)
+        for s in self.streams:
+            s.wait_event(start)
+        for i, cam in enumerate(cams):
+            k = i % self.depth
+            p, s = self.pipes[k], self.streams[k]
+            p.build(xyz, cam, s)
+            p.sample(xyz, cam, s)
+            if on_view is not None:
+                on_view(i, p, s)
+        for s in self.streams:
+            done = torch.cuda.Event()
+            done.record(s)
+            main.wait_event(done)

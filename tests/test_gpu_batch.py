@@ -139,3 +139,30 @@ def test_view_pipeline_tune_keeps_outputs():
     torch.cuda.synchronize()
     for a, b in zip(before, after):
         assert torch.equal(a.view(torch.uint8), b.view(torch.uint8))
+
+
+def test_view_ring_matches_one_stream():
+    """ViewRing (per-view launches over 3 streams, a buffer set each) gives every view the outputs
+    of the same launches one after another on one stream; on_view sees each view's outputs before
+    its buffers are reused."""
+    from hashpoint.engine import CameraTable, ViewPipeline, ViewRing
+    sc = synth.make_shapes(n=60000, n_views=7, width=160, height=128, f=220.0, with_feat=False)
+    X = torch.from_numpy(sc.xyz).cuda()
+    cams = CameraTable(sc.cameras, "cuda")
+    structs = [cams.struct(i) for i in range(cams.n)]
+    pipe = ViewPipeline(len(sc.xyz), 128, 160, sc.options, "cuda")
+    ref = [[t.clone() for t in pipe.render(X, s)] for s in structs]
+    ring = ViewRing(len(sc.xyz), 128, 160, sc.options, "cuda", depth=3)
+    got = [None] * len(structs)
+
+    def keep(i, p, stream):
+        with torch.cuda.stream(stream):
+            got[i] = [t.clone() for t in (p.sp_xyz, p.pc_idx, p.sp_t, p.mask)]
+
+    main = torch.cuda.current_stream()
+    ring.render_many(X, structs, main, on_view=keep)
+    torch.cuda.synchronize()
+    for a_view, b_view in zip(ref, got):
+        for a, b in zip(a_view, b_view):
+            assert torch.equal(a.view(torch.uint8), b.view(torch.uint8))
+    assert any(bool(v[3].any()) for v in got)
