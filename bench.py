@@ -234,7 +234,7 @@ def run_gpu(args):
 
     # the sampling kernel's stage configuration for this workload (outputs never depend on it)
     with torch.cuda.stream(stream):
-        stage = ring.tune(xyz, structs[:5], stream)
+        stage = ring.tune(xyz, structs[:12], stream)
 
     # in-image point count per view (for the algorithmic byte count), outside timing
     n_in = []

@@ -143,10 +143,27 @@ class ViewRing:
             p.tuning = tuning
 
     def tune(self, xyz, cams, stream=None, reps=2):
-        """ViewPipeline.tune on the first pipeline; every pipeline then uses its choice."""
-        cfg = self.pipes[0].tune(xyz, cams, stream, reps)
-        self.set_tuning(self.pipes[0].tuning)
-        return cfg
+        """Pick the stage configuration of the sampling kernel for this shape by timing
+        render_many over `cams` in each (CUDA events on `stream`): with launches overlapping
+        across streams, the fastest configuration can differ from the one-stream choice
+        (ViewPipeline.tune).  Outputs never depend on it."""
+        main = stream or torch.cuda.current_stream(self.device)
+        best = None
+        for cfg in native.STAGE_CONFIGS:
+            self.set_tuning(make_tuning(stage_config=cfg))
+            ms = []
+            for rep in range(reps + 1):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(main)
+                self.render_many(xyz, cams, main)
+                e1.record(main)
+                e1.synchronize()
+                if rep:  # the first pass loads and warms the configuration's kernels
+                    ms.append(e0.elapsed_time(e1))
+            if best is None or min(ms) < best[0]:
+                best = (min(ms), cfg)
+        self.set_tuning(make_tuning(stage_config=best[1]))
+        return best[1]
 
     def render_many(self, xyz, cams, stream=None, on_view=None):
         """Render `cams` (HpCamera structs); the views' work starts after, and `stream` waits for,

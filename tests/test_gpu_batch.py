@@ -153,6 +153,8 @@ def test_view_ring_matches_one_stream():
     pipe = ViewPipeline(len(sc.xyz), 128, 160, sc.options, "cuda")
     ref = [[t.clone() for t in pipe.render(X, s)] for s in structs]
     ring = ViewRing(len(sc.xyz), 128, 160, sc.options, "cuda", depth=3)
+    cfg = ring.tune(X, structs, reps=1)
+    assert cfg in native.STAGE_CONFIGS and all(p.tuning.stage_config == cfg for p in ring.pipes)
     got = [None] * len(structs)
 
     def keep(i, p, stream):
