@@ -969,9 +969,21 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
       }
 #pragma unroll
       for (int q = 0; q < kBallPass; q++) {
-        // once the buffer is full and has had a replacement, maxd is its true
-        // maximum and only decreases, so hits at or beyond it cannot change it
-        unsigned mm = __ballot_sync(kAll, hq[q] && (!settled[q] || dq[q] < maxd[q]));
+        // Which of the chunk's hits can change the buffer (bsize, settled and
+        // maxd are the same in every lane).  While filling: all of them.  Once
+        // full and replaced at least once, maxd is the buffer's true maximum and
+        // only decreases, so only hits below it.  Full but never replaced, maxd
+        // is the minimum of the first eight (the reference's quirk) and the
+        // buffer stays as it is until a hit falls below it; from that hit on,
+        // maxd becomes the true maximum, so every later hit is looked at.
+        unsigned mm;
+        if (bsize[q] < kBallBuf || settled[q]) {
+          mm = __ballot_sync(kAll, hq[q] && (bsize[q] < kBallBuf || dq[q] < maxd[q]));
+        } else {
+          const unsigned first = __ballot_sync(kAll, hq[q] && dq[q] < maxd[q]);
+          const unsigned all = __ballot_sync(kAll, hq[q]);
+          mm = first ? all & ~((1u << (__ffs(first) - 1)) - 1u) : 0u;
+        }
         while (mm) {
           const int l = __ffs(mm) - 1;
           mm &= mm - 1;
