@@ -104,12 +104,16 @@ struct StageCfg {
   static constexpr int kItemsPerTile = kTileH * 4;  // rows, each in up to four column quarters
   static_assert((kThreads == 256 || kThreads == 128) && kTileW >= 4 && kTileW <= 32 && kTileH <= 16, "tile shape");
 };
-using Cfg2560x4 = StageCfg<2560, 4, 8, 32>;     // 40 KB stage, 4 blocks per SM, 8 x 32 tiles (the default)
+using Cfg2560x4 = StageCfg<2560, 4, 8, 32>;     // 40 KB stage, 4 blocks per SM, 8 x 32 tiles
 using Cfg3712x3 = StageCfg<3712, 3, 8, 32>;     // 58 KB stage, 3 blocks per SM
 using Cfg5888x2 = StageCfg<5888, 2, 8, 32>;     // 92 KB stage, 2 blocks per SM
 using Cfg2560x4Sq = StageCfg<2560, 4, 16, 16>;  // 16 x 16 tiles
 using Cfg3712x3Sq = StageCfg<3712, 3, 16, 16>;
-constexpr int kStageConfigs = 5;      // hp_tuning.stage_config 1..5 (0 = the default, 1)
+constexpr int kStageConfigs = 5;      // hp_tuning.stage_config 1..5 (0 = the default)
+// The default: 16 x 16 tiles with 2560 staged points x 4 blocks, measured
+// fastest or level on the shapes, clustered and multi-view workloads (the
+// small sphere view prefers 5888 x 2, which a tuner finds).
+constexpr int kDefaultStageConfig = 4;
 constexpr int kMaxItemsPerTile = 64;  // over the configurations (16 rows, four column ranges each)
 constexpr int kCellsPerThread = 2;    // halo cells per thread (<= 432 = the largest halo)
 
@@ -1656,7 +1660,7 @@ int32_t sampling_grid(int config, int* blocks, int* sm_count = nullptr) {
 
 // Launch tuning shared by both entry points; outputs never depend on it.
 struct Tune {
-  int heavy = kHeavyWindow, per_sm = 0, config = 1;
+  int heavy = kHeavyWindow, per_sm = 0, config = kDefaultStageConfig;
 };
 
 static int32_t read_tuning(const char* who, const hp_tuning* tuning, Tune& t) {
@@ -1795,7 +1799,7 @@ static int32_t check_sampling(const char* who, const float* xyz, int64_t n_point
 
 extern "C" int32_t hp_stage_config_info(int32_t config, int32_t* tile_h, int32_t* tile_w, int32_t* stage_points,
                                         int32_t* blocks_per_sm) {
-  if (config == 0) config = 1;
+  if (config == 0) config = kDefaultStageConfig;
   if (config < 1 || config > kStageConfigs)
     return set_error(HP_ERR_INVALID_ARGUMENT, "hp_stage_config_info: stage_config %d outside 0..%d", config,
                      kStageConfigs);

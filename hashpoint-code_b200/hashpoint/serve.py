@@ -229,6 +229,22 @@ class Server:
             ws = self.build_ws[slot] = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=self.device)
         return ws
 
+    def tune(self, requests, tuner=None):
+        """Pick the batch launch tuning (stage configuration, heavy-ray threshold) on a sample of
+        requests, as a service would once at start-up: hashpoint.batch.Autotuner over one batch of
+        their views.  Returns (stage_config, heavy_window); outputs never depend on it."""
+        from . import batch
+        views = []
+        for r in requests[: self.max_views]:
+            cam, _, _, _ = self.store.camera(r.scene, r.pose, r.width, r.height)
+            views.append((r.scene, cam))
+        renderer = batch.BatchRenderer(self.store.clouds, views, self.store.options, self.device)
+        choice = (tuner or batch.Autotuner(reps=1)).tune(renderer)
+        self.tuning = renderer.tuning
+        del renderer
+        torch.cuda.empty_cache()
+        return choice
+
     def _bytes_needed(self, req):
         return output_bytes(req, self.store.options) + self.store.entry_bytes(req)
 

@@ -241,7 +241,7 @@ HP_API size_t hp_quick_sampling_workspace_size(int64_t n_sorted, int32_t height,
  *                  whole warp instead of one thread (0..4096; default 320).
  *   blocks_per_sm  resident blocks of the persistent sampling kernel per SM
  *                  (default: as many as fit).
- *   stage_config   stage and tile of the sampling kernel (0 = 1):
+ *   stage_config   stage and tile of the sampling kernel (0 = 4):
  *                  1: 2560 staged points per tile, 4 blocks per SM, 8 x 32 tiles;
  *                  2: 3712 points, 3 blocks per SM, 8 x 32;
  *                  3: 5888 points, 2 blocks per SM, 8 x 32;
@@ -256,7 +256,7 @@ typedef struct hp_tuning {
 } hp_tuning;
 
 /* The tile (tile_h x tile_w pixels), staged points per tile and resident
- * blocks per SM of a stage configuration (0 reads as 1); any output pointer
+ * blocks per SM of a stage configuration (0 reads as 4); any output pointer
  * may be NULL.  HP_ERR_INVALID_ARGUMENT outside 0..5.  No counterpart in the
  * reference. */
 HP_API int32_t hp_stage_config_info(int32_t config, int32_t* tile_h, int32_t* tile_w, int32_t* stage_points,

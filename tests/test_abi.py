@@ -168,7 +168,7 @@ def test_batch_workspace_and_validation(L):
 
 def test_stage_config_info(L):
     shapes = {c: native.stage_config_info(c) for c in native.STAGE_CONFIGS}
-    assert native.stage_config_info(0) == shapes[1]
+    assert native.stage_config_info(0) == shapes[4]  # the default
     for c, d in shapes.items():
         assert d["tile_h"] * d["tile_w"] == 256 and d["stage_points"] > 0 and d["blocks_per_sm"] >= 1
     assert {(d["tile_h"], d["tile_w"]) for d in shapes.values()} == {(8, 32), (16, 16)}

@@ -61,6 +61,8 @@ def test_served_results_equal_alone(store):
     reqs = serve.poisson_requests(rng, 48, 20000.0, 3, 4, RES)
     got, on_result = _collect()
     srv = serve.Server(store, 8 << 30, streams=3, max_views=8, on_result=on_result)
+    stage, heavy = srv.tune(reqs[:8])  # start-up tuning; results must not depend on it
+    assert srv.tuning.stage_config == stage and srv.tuning.heavy_window == heavy
     stats = srv.run(reqs)
     assert stats["done"] == 48 and stats["rejected"] == 0
     assert stats["batches"] < 48  # requests were batched
