@@ -32,6 +32,9 @@
 #include <mutex>
 
 #include "hp_common.cuh"
+#ifdef HP_TESTING
+#include "../../include/hashpoint_b200_testing.h"
+#endif
 
 namespace hp {
 
@@ -148,15 +151,17 @@ __device__ __forceinline__ int block_reduce_sum(int v, int* sh) {
 // the totals of all earlier tiles (a look-back over totals alone: no tile
 // waits on another's running total, so there is no chain), and the tile scans
 // its run chunk by chunk from that carry.  Every poll of an earlier tile is
-// bounded (kLookBackSpins); a tile that gives up counts that tile as empty
-// and sets scalars[3] (the table is then wrong; this does not happen while
-// the tiles it waits on are running).  Also lists the pixels whose
+// bounded (`spins` polls, kLookBackSpins in the product); a tile that gives up
+// counts that tile as empty and sets scalars[3], which hp_pts2plane_status
+// reports (the table is then wrong; this does not happen while the tiles it
+// waits on are running).  `withhold` >= 0 names a tile that never publishes
+// its total, so that a test can make the others give up.  Also lists the pixels whose
 // buckets exceed kRankMax (count in scalars[1]), for k_sort_huge_list.
 // scalars[2]: the tile counter; scalars[0]: the points inside the image.
 __global__ void __launch_bounds__(kScanThreads) k_scan_hash(const int* __restrict__ counts, int hw, int chunks_per_tile,
                                                             unsigned long long* __restrict__ look,
                                                             int2* __restrict__ hash, int* __restrict__ scalars,
-                                                            int* __restrict__ huge) {
+                                                            int* __restrict__ huge, int withhold, int spins) {
   __shared__ int sh[32];
   __shared__ int warp_tot[32];
   __shared__ int s_tile, s_carry;
@@ -187,12 +192,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_hash(const int* __restric
   }
   const int total = block_reduce_sum(part, sh);
   if (warp == 0) {
-    if (lane == 0) atomicExch(look + tile, kAggregate | (unsigned)total);
+    if (lane == 0 && tile != withhold) atomicExch(look + tile, kAggregate | (unsigned)total);
     int carry = 0;
     for (int q = lane; q < tile; q += 32) {
       unsigned long long f = *(volatile unsigned long long*)(look + q);
       for (int spin = 0; (f >> 62) == 0; spin++) {
-        if (spin == kLookBackSpins) {
+        if (spin == spins) {
           atomicExch(scalars + 3, 1);
           f = kAggregate;  // counted as empty
           break;
@@ -347,6 +352,9 @@ __global__ void __launch_bounds__(256) k_order(Entries in, const int2* __restric
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_in; j += gridDim.x * blockDim.x) {
     int2 h, e;
     if (!in.entry(j, hash, hw, h, e)) continue;
+    // a bucket inside [0, n_in) -- always, unless the scan gave up waiting (hp_pts2plane_status),
+    // when the scratch may hold records no point wrote: then outputs are wrong but stay in bounds
+    if (h.x < 0 || h.y < 1 || h.y > n_in - h.x) continue;
     if (h.y > kRankMax) continue;
     const float d = __int_as_float(e.y);
     int pos = h.x;
@@ -565,9 +573,10 @@ extern "C" size_t hp_pts2plane_workspace_size(int64_t n_points, int32_t height, 
   return build_layout(n_points, (int64_t)height * width).total;
 }
 
-extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_camera* cam, int32_t sort,
-                                int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table, void* workspace,
-                                size_t workspace_bytes, hp_stream_t stream) {
+// hp_pts2plane with the scan's test hooks (withhold: see k_scan_hash).
+static int32_t pts2plane(const float* xyz, int64_t n_points, const hp_camera* cam, int32_t sort,
+                         int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table, void* workspace,
+                         size_t workspace_bytes, hp_stream_t stream, int withhold, int spins) {
   if (!cam) return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane: cam is NULL");
   const int H = cam->height, W = cam->width;
   if (H <= 0 || W <= 0 || (int64_t)H * W >= (1ll << 31))
@@ -609,7 +618,7 @@ extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_cam
   const int nchunks = (int)((hw + kScanTile - 1) / kScanTile);
   const int per_tile = (nchunks + kScanMaxTiles - 1) / kScanMaxTiles;
   const int tiles = (nchunks + per_tile - 1) / per_tile;
-  k_scan_hash<<<tiles, kScanThreads, 0, st>>>(counts, (int)hw, per_tile, look, hash, scalars, huge);
+  k_scan_hash<<<tiles, kScanThreads, 0, st>>>(counts, (int)hw, per_tile, look, hash, scalars, huge, withhold, spins);
   if (int32_t rc = check_launch("k_scan_hash")) return rc;
   if (n > 0) {
     k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, (int)hw, pid_slot, depth, hash, scalars, tmp,
@@ -619,6 +628,39 @@ extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_cam
   return launch_order((int)hw, -1, n, PackedEntries{tmp}, hash, scalars, huge, sorted_point_idx, sorted_depth,
                       BucketOrder{sort != 0, 0}, st);
 }
+
+extern "C" int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_camera* cam, int32_t sort,
+                                int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table, void* workspace,
+                                size_t workspace_bytes, hp_stream_t stream) {
+  return pts2plane(xyz, n_points, cam, sort, sorted_point_idx, sorted_depth, hash_table, workspace, workspace_bytes,
+                   stream, -1, kLookBackSpins);
+}
+
+extern "C" int32_t hp_pts2plane_status(const void* workspace, int64_t n_points, int32_t height, int32_t width,
+                                       hp_stream_t stream) {
+  if (!workspace || n_points < 0 || height <= 0 || width <= 0)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane_status: bad arguments");
+  const BuildLayout L = build_layout(n_points, (int64_t)height * width);
+  int flag = 0;
+  if (cudaMemcpyAsync(&flag, (const char*)workspace + L.scalars + 3 * sizeof(int), sizeof(int),
+                      cudaMemcpyDeviceToHost, (cudaStream_t)stream) != cudaSuccess ||
+      cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
+    return set_error(HP_ERR_CUDA, "hp_pts2plane_status: %s", cudaGetErrorString(cudaGetLastError()));
+  if (flag) return set_error(HP_ERR_CUDA, "hp_pts2plane: the hash-table scan gave up waiting for a block");
+  return HP_OK;
+}
+
+#ifdef HP_TESTING
+extern "C" int32_t hp_pts2plane_withheld(const float* xyz, int64_t n_points, const hp_camera* cam, int32_t sort,
+                                         int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table,
+                                         void* workspace, size_t workspace_bytes, int32_t withhold_tile,
+                                         hp_stream_t stream) {
+  if (withhold_tile < 0)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane_withheld: withhold_tile must be >= 0");
+  return pts2plane(xyz, n_points, cam, sort, sorted_point_idx, sorted_depth, hash_table, workspace, workspace_bytes,
+                   stream, withhold_tile, 1024);
+}
+#endif
 
 extern "C" int32_t hp_scatter_hashtable(const int32_t* point_idx, const int32_t* point2img, const float* depth,
                                         int64_t n, int32_t height, int32_t width, int32_t sort,

@@ -32,21 +32,22 @@ SOURCES = ["hp_api.cu", "hp_build.cu", "hp_sample.cu", "hp_query.cu", "hp_featur
 # wait-expiry test of the Aggregator, compiled with the sources they exercise; never loaded by the product.
 TESTING_LIB_NAME = "libhashpoint_b200_testing.so"
 TESTING_LIB_PATH = os.path.join(LIB_DIR, TESTING_LIB_NAME)
-TESTING_SOURCES = ["hp_api.cu", "hp_aggregator.cu", "hp_tc_check.cu"]
+TESTING_SOURCES = ["hp_api.cu", "hp_build.cu", "hp_aggregator.cu", "hp_tc_check.cu"]
 TESTING_FLAGS = ["-DHP_TESTING"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 
 # C-ABI symbols declared in include/hashpoint_b200.h
 EXPORTS = ["hp_version", "hp_last_error", "hp_projection_rounding", "hp_pts2plane_workspace_size", "hp_pts2plane",
-           "hp_pts2plane_noalloc", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling",
+           "hp_pts2plane_noalloc", "hp_pts2plane_status", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling",
            "hp_quick_sampling_tuned", "hp_stage_config_info",
            "hp_quick_sampling_batch_workspace_size", "hp_quick_sampling_batch", "hp_quick_query_for_nearby_point",
            "hp_scatter", "hp_ray_directions", "hp_mask_scan", "hp_mask_scan_workspace_size", "hp_feature_query",
            "hp_clamp_t", "hp_render", "hp_aggregator_packed_size", "hp_aggregator_pack",
            "hp_aggregator_workspace_size", "hp_aggregator_forward", "hp_aggregator_status"]
 # declared in include/hashpoint_b200_testing.h, exported by the test-only library
-TESTING_EXPORTS = ["hp_tc_check_image_bytes", "hp_tc_check_mma", "hp_aggregator_forward_withheld"]
+TESTING_EXPORTS = ["hp_tc_check_image_bytes", "hp_tc_check_mma", "hp_aggregator_forward_withheld",
+                   "hp_pts2plane_withheld"]
 
 HP_OK = 0
 
@@ -230,6 +231,8 @@ def lib():
         L.hp_pts2plane.restype = i32
         L.hp_pts2plane_noalloc.argtypes = [vp, i64, cam_p, i32, vp, vp, vp, vp]
         L.hp_pts2plane_noalloc.restype = i32
+        L.hp_pts2plane_status.argtypes = [vp, i64, i32, i32, vp]
+        L.hp_pts2plane_status.restype = i32
         L.hp_scatter_hashtable.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp, vp]
         L.hp_scatter_hashtable.restype = i32
         L.hp_quick_sampling_workspace_size.argtypes = [i64, i32, i32]
@@ -305,6 +308,13 @@ def testing_lib():
         T.hp_aggregator_forward_withheld.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp, vp, i64, i32, vp, vp, i64, vp,
                                                      vp, vp, sz, i32, vp]
         T.hp_aggregator_forward_withheld.restype = i32
+        cam_p = ctypes.POINTER(HpCamera)
+        T.hp_pts2plane_workspace_size.argtypes = [i64, i32, i32]
+        T.hp_pts2plane_workspace_size.restype = sz
+        T.hp_pts2plane_withheld.argtypes = [vp, i64, cam_p, i32, vp, vp, vp, vp, sz, i32, vp]
+        T.hp_pts2plane_withheld.restype = i32
+        T.hp_pts2plane_status.argtypes = [vp, i64, i32, i32, vp]
+        T.hp_pts2plane_status.restype = i32
         _testing = T
         return _testing
 

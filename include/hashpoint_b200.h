@@ -97,6 +97,15 @@ HP_API int32_t hp_pts2plane(const float* xyz, int64_t n_points, const hp_camera*
                      int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table,
                      void* workspace, size_t workspace_bytes, hp_stream_t stream);
 
+/* Reports whether the hash-table scan of the last hp_pts2plane on this
+ * workspace (same n_points, height and width) had to give up waiting for one
+ * of its blocks (its waits are bounded; the table is then wrong): HP_OK, or
+ * HP_ERR_CUDA with the reason in hp_last_error().  Synchronises on stream.
+ * This does not happen while the GPU runs the call's blocks; the check exists
+ * so that a failure would be seen.  No counterpart in the reference. */
+HP_API int32_t hp_pts2plane_status(const void* workspace, int64_t n_points, int32_t height, int32_t width,
+                                   hp_stream_t stream);
+
 /* hp_pts2plane for callers that cannot allocate device memory: a host plugin
  * that only receives device pointers for its inputs and outputs from the
  * application embedding it, or a service that must not grow its device

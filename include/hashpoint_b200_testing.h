@@ -50,6 +50,16 @@ HP_API int32_t hp_aggregator_forward_withheld(const void* packed, const float* p
                                               float* color_out, void* workspace, size_t workspace_bytes,
                                               int32_t wait_limit_us, hp_stream_t stream);
 
+/* A test of the hash-table scan's bounded waits: hp_pts2plane with the scan
+ * block that starts withhold_tile-th never publishing its total.  The blocks
+ * after it poll it a bounded number of times, give up, count it as empty and
+ * flag the failure, which hp_pts2plane_status reports; the outputs are not
+ * valid.  The context stays usable. */
+HP_API int32_t hp_pts2plane_withheld(const float* xyz, int64_t n_points, const hp_camera* cam, int32_t sort,
+                                     int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table,
+                                     void* workspace, size_t workspace_bytes, int32_t withhold_tile,
+                                     hp_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

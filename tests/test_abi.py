@@ -180,6 +180,13 @@ def test_stage_config_info(L):
         assert "stage_config" in _err(L)
 
 
+def test_pts2plane_status_validation(L):
+    assert L.hp_pts2plane_status(None, 10, 8, 8, None) == -1
+    assert L.hp_pts2plane_status(ctypes.c_void_p(0x1000), -1, 8, 8, None) == -1
+    assert L.hp_pts2plane_status(ctypes.c_void_p(0x1000), 10, 0, 8, None) == -1
+    assert "bad arguments" in _err(L)
+
+
 def test_pts2plane_checks_workspace(L):
     p = ctypes.c_void_p(0x1000)
     need = L.hp_pts2plane_workspace_size(10, 8, 8)

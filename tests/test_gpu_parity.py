@@ -302,6 +302,37 @@ def test_epcq_camera_scalars_on_the_device():
     assert outs[0][-1].any()
 
 
+def test_scan_wait_gives_up_and_reports():
+    """The hash-table scan's waits are bounded: with one scan block withheld (test library), the
+    blocks after it give up, hp_pts2plane_status reports it, and the next plain call on the same
+    workspace and context is correct again and reports nothing."""
+    import ctypes
+    native.build_testing()
+    T, L = native.testing_lib(), native.lib()
+    rng = np.random.default_rng(41)
+    xyz = synth.shapes_cloud(rng, 20000)
+    cam = synth.orbit_cameras(rng, 1, 4.0, 160, 128, 180.0)[0]  # 20480 pixels: five 4096-pixel scan blocks
+    n, Hh, W = len(xyz), cam.height, cam.width
+    X, w2c, K = D(xyz), D(cam.w2c), D(cam.K)  # kept alive: the camera struct holds their device pointers
+    hc = ops.make_camera(w2c=w2c, K=K, width=W, height=Hh)
+    ws_bytes = L.hp_pts2plane_workspace_size(n, Hh, W)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    sidx = torch.empty(n, dtype=torch.int32, device="cuda")
+    sdep = torch.empty(n, dtype=torch.float32, device="cuda")
+    hsh = torch.empty((Hh * W, 2), dtype=torch.int32, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ptrs = [ctypes.c_void_p(t.data_ptr()) for t in (sidx, sdep, hsh, ws)]
+    rc = T.hp_pts2plane_withheld(ctypes.c_void_p(X.data_ptr()), n, ctypes.byref(hc), 0, *ptrs, ws_bytes, 0, stream)
+    native.check(rc, "hp_pts2plane_withheld", T)
+    assert T.hp_pts2plane_status(ptrs[3], n, Hh, W, stream) != 0
+    assert "gave up" in T.hp_last_error().decode()
+    rc = L.hp_pts2plane(ctypes.c_void_p(X.data_ptr()), n, ctypes.byref(hc), 0, *ptrs, ws_bytes, stream)
+    native.check(rc, "hp_pts2plane")
+    native.check(L.hp_pts2plane_status(ptrs[3], n, Hh, W, stream), "hp_pts2plane_status")
+    oi, od, oh = O.pts2plane(xyz, O.camera_from(cam), False)
+    assert np.array_equal(H(hsh), oh) and np.array_equal(H(sidx), oi) and np.array_equal(bits(H(sdep)), bits(od))
+
+
 def test_repeatable():
     xyz, cam, opt, sort = _case(*CASES["clusters_192x160_k5_S16"])
     a = _run_case(xyz, cam, opt, sort)
