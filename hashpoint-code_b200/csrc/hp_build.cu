@@ -752,3 +752,21 @@ extern "C" int32_t hp_pts2plane_noalloc(const float* xyz, int64_t n_points, cons
   return hp_pts2plane(xyz, n_points, cam, sort, sorted_point_idx, sorted_depth, hash_table, scratch,
                       kNoAllocScratchBytes, stream);
 }
+
+extern "C" int32_t hp_pts2plane_noalloc_status(int64_t n_points, int32_t height, int32_t width, hp_stream_t stream) {
+  if (n_points < 0 || n_points > kNoAllocMaxPoints || height <= 0 || width <= 0 ||
+      (int64_t)height * width > kNoAllocMaxPixels)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane_noalloc_status: bad arguments");
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
+    return set_error(HP_ERR_CUDA, "hp_pts2plane_noalloc_status: no usable device");
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    scratch = g_noalloc_addr[dev];
+  }
+  if (!scratch)
+    return set_error(HP_ERR_INVALID_ARGUMENT, "hp_pts2plane_noalloc_status: no hp_pts2plane_noalloc call on device %d",
+                     dev);
+  return hp_pts2plane_status(scratch, n_points, height, width, stream);
+}

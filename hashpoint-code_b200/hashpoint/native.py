@@ -39,7 +39,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
 
 # C-ABI symbols declared in include/hashpoint_b200.h
 EXPORTS = ["hp_version", "hp_last_error", "hp_projection_rounding", "hp_pts2plane_workspace_size", "hp_pts2plane",
-           "hp_pts2plane_noalloc", "hp_pts2plane_status", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling",
+           "hp_pts2plane_noalloc", "hp_pts2plane_status", "hp_pts2plane_noalloc_status", "hp_scatter_hashtable", "hp_quick_sampling_workspace_size", "hp_quick_sampling",
            "hp_quick_sampling_tuned", "hp_stage_config_info",
            "hp_quick_sampling_batch_workspace_size", "hp_quick_sampling_batch", "hp_quick_query_for_nearby_point",
            "hp_scatter", "hp_ray_directions", "hp_mask_scan", "hp_mask_scan_workspace_size", "hp_feature_query",
@@ -233,6 +233,8 @@ def lib():
         L.hp_pts2plane_noalloc.restype = i32
         L.hp_pts2plane_status.argtypes = [vp, i64, i32, i32, vp]
         L.hp_pts2plane_status.restype = i32
+        L.hp_pts2plane_noalloc_status.argtypes = [i64, i32, i32, vp]
+        L.hp_pts2plane_noalloc_status.restype = i32
         L.hp_scatter_hashtable.argtypes = [vp, vp, vp, i64, i32, i32, i32, vp, vp, vp, vp]
         L.hp_scatter_hashtable.restype = i32
         L.hp_quick_sampling_workspace_size.argtypes = [i64, i32, i32]

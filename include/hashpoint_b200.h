@@ -129,6 +129,10 @@ HP_API int32_t hp_pts2plane_noalloc(const float* xyz, int64_t n_points, const hp
                                     int32_t* sorted_point_idx, float* sorted_depth, int32_t* hash_table,
                                     hp_stream_t stream);
 
+/* hp_pts2plane_status for the last hp_pts2plane_noalloc on the current
+ * device (same n_points, height and width).  Synchronises on stream. */
+HP_API int32_t hp_pts2plane_noalloc_status(int64_t n_points, int32_t height, int32_t width, hp_stream_t stream);
+
 /* Per-pixel hash table from inputs already sorted by pixel id.  Replaces
  * _C.scatter_hashtable (epcq/csrc/rasterization.cu:130-171, kernel :7-34):
  * point_idx / point2img / depth [n] sorted by point2img ascending; entries with

@@ -185,6 +185,8 @@ def test_pts2plane_status_validation(L):
     assert L.hp_pts2plane_status(ctypes.c_void_p(0x1000), -1, 8, 8, None) == -1
     assert L.hp_pts2plane_status(ctypes.c_void_p(0x1000), 10, 0, 8, None) == -1
     assert "bad arguments" in _err(L)
+    assert L.hp_pts2plane_noalloc_status(262145, 8, 8, None) == -1
+    assert L.hp_pts2plane_noalloc_status(10, 1025, 1024, None) == -1
 
 
 def test_pts2plane_checks_workspace(L):

@@ -37,6 +37,7 @@ def _noalloc(xyz, w2c, K, height, width, sort):
                                 ctypes.c_void_p(sidx.data_ptr()), ctypes.c_void_p(sdep.data_ptr()),
                                 ctypes.c_void_p(hsh.data_ptr()), stream)
     native.check(rc, "hp_pts2plane_noalloc")
+    native.check(L.hp_pts2plane_noalloc_status(n, height, width, stream), "hp_pts2plane_noalloc_status")
     return sidx, sdep, hsh
 
 
