@@ -222,6 +222,81 @@ __global__ void __launch_bounds__(256) k_feature_query(FeatArgs a) {
   }
 }
 
+// The same gather with 16-byte moves, for feature rows whose bytes are a
+// multiple of 16 (F = 32 fp16 or fp32 features, the Aggregator's width): per
+// valid sample every lane moves 16-byte chunks of the feature rows (fp16
+// chunks widened to two float4 stores), so a sample's features take one
+// gather round instead of one per 32-element pass.
+template <int kHalf>
+__global__ void __launch_bounds__(256) k_feature_query_vec(FeatArgs a) {
+  constexpr int kEsz = kHalf ? 2 : 4;
+  const int lane = threadIdx.x & 31;
+  const int64_t i0 = ((int64_t)blockIdx.x * 8 + (threadIdx.x >> 5)) * 32;
+  if (i0 >= a.n_samples) return;
+  const int64_t my = i0 + lane;
+  const bool valid = my < a.n_samples && a.mask[my] != 0;
+  unsigned todo = __ballot_sync(0xffffffffu, valid);
+  const int my_off = valid ? a.offsets[my] : 0;
+  const int P = a.P, F = a.feat_dim;
+  const int cpp = F * kEsz / 16;  // 16-byte chunks per feature row
+  const char* feat = reinterpret_cast<const char*>(a.feat);
+  auto one = [&](int l) {
+    const int64_t i = i0 + l;
+    const int64_t m = __shfl_sync(0xffffffffu, my_off, l);
+    const int64_t ray = i / a.S;
+    const int* ids = a.pc_idx + i * P;  // the same few words for every lane (L1)
+    if (lane < 3) a.o_sp[m * 3 + lane] = a.sp_xyz[i * 3 + lane];
+    if (lane >= 3 && lane < 6) {
+      const int c = lane - 3;
+      int u, v;
+      if (a.ray_uv) {
+        u = a.ray_uv[2 * ray];
+        v = a.ray_uv[2 * ray + 1];
+      } else {
+        u = (int)(ray % a.width);
+        v = (int)(ray / a.width);
+      }
+      const float dx = __fdiv_rn(__fsub_rn((float)u, a.cx), a.fx);
+      const float dy = __fdiv_rn(__fsub_rn((float)v, a.cy), a.fy);
+      const float* R = a.c2w + 4 * c;
+      a.o_rays[m * 3 + c] = __fadd_rn(__fadd_rn(__fmul_rn(dx, R[0]), __fmul_rn(dy, R[1])), R[2]);
+    }
+    for (int e = lane; e < 3 * P; e += 32) {
+      const int p = e / 3, c = e - 3 * p;
+      const int id = ids[p];
+      const bool ok = (unsigned)id < (unsigned)a.n_points;
+      if (c == 0) a.o_valid[m * P + p] = ok;
+      const int64_t o = (m * P + p) * 3 + c;
+      a.o_xyz[o] = ok ? a.xyz[(int64_t)id * 3 + c] : 0.0f;
+      a.o_rgb[o] = ok ? a.rgb[(int64_t)id * 3 + c] : 0.0f;
+      a.o_dir[o] = ok ? a.dir[(int64_t)id * 3 + c] : 0.0f;
+    }
+    float* of = a.o_feat + m * P * F;
+    for (int c = lane; c < P * cpp; c += 32) {
+      const int p = c / cpp, q = c - p * cpp;
+      const int id = ids[p];
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if ((unsigned)id < (unsigned)a.n_points)
+        v = __ldg(reinterpret_cast<const uint4*>(feat + ((int64_t)id * cpp + q) * 16));
+      if constexpr (kHalf) {
+        const __half2* h = reinterpret_cast<const __half2*>(&v);
+        const float2 f0 = __half22float2(h[0]), f1 = __half22float2(h[1]), f2 = __half22float2(h[2]),
+                     f3 = __half22float2(h[3]);
+        float4* dst = reinterpret_cast<float4*>(of + p * F + q * 8);
+        dst[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
+        dst[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
+      } else {
+        *reinterpret_cast<uint4*>(of + p * F + q * 4) = v;
+      }
+    }
+  };
+  while (todo) {
+    const int l = __ffs(todo) - 1;
+    todo &= todo - 1;
+    one(l);
+  }
+}
+
 // clamp_t: gaps outside (1e-8, 2 vsize], and the last sample's, become vsize.
 __device__ __forceinline__ float clamped_gap(const float* t, int s, int S, float vsize) {
   const float d = s + 1 < S ? __fsub_rn(t[s + 1], t[s]) : vsize;
@@ -343,7 +418,16 @@ extern "C" int32_t hp_feature_query(const hp_point_attrs* pts, const float* sp_x
   a.o_valid = valid;
   a.o_rays = rays_d;
   const int64_t warps = (a.n_samples + 31) / 32;
-  k_feature_query<<<(unsigned)((warps + 7) / 8), 256, 0, (cudaStream_t)stream>>>(a);
+  const int esz = a.feat_half ? 2 : 4;
+  // 16-byte moves when the rows and both base addresses allow them
+  const bool vec = a.feat_dim > 0 && (a.feat_dim * esz) % 16 == 0 && ((uintptr_t)a.feat & 15) == 0 &&
+                   ((uintptr_t)a.o_feat & 15) == 0;
+  if (vec && a.feat_half)
+    k_feature_query_vec<1><<<(unsigned)((warps + 7) / 8), 256, 0, (cudaStream_t)stream>>>(a);
+  else if (vec)
+    k_feature_query_vec<0><<<(unsigned)((warps + 7) / 8), 256, 0, (cudaStream_t)stream>>>(a);
+  else
+    k_feature_query<<<(unsigned)((warps + 7) / 8), 256, 0, (cudaStream_t)stream>>>(a);
   return check_launch("k_feature_query");
 }
 
