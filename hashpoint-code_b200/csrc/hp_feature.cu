@@ -338,6 +338,52 @@ __global__ void k_render(const float* __restrict__ deltas, const float* __restri
   color[r * 3 + 2] = __fadd_rn(c2, __fmul_rn(bg_trans, bg));
 }
 
+// The same for S = kS (a multiple of 4) with 16-byte aligned bases: a ray's
+// sigma, t (or delta) and rgb rows are loaded as 16-byte vectors before any
+// arithmetic, so a thread waits on one round of loads instead of one per
+// sample; the arithmetic and its order are k_render's.
+template <int kS>
+__global__ void __launch_bounds__(256) k_render_vec(const float* __restrict__ deltas, const float* __restrict__ t_val,
+                                                    float vsize, const float* __restrict__ sigmas,
+                                                    const float* __restrict__ rgbs, int64_t rays, int white_bg,
+                                                    float* __restrict__ color) {
+  static_assert(kS % 4 == 0, "kS must be a multiple of 4");
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rays) return;
+  float sg[kS], tv[kS], cl[3 * kS];
+  const float4* s4 = reinterpret_cast<const float4*>(sigmas + r * kS);
+  const float4* t4 = reinterpret_cast<const float4*>((deltas ? deltas : t_val) + r * kS);
+  const float4* c4 = reinterpret_cast<const float4*>(rgbs + r * kS * 3);
+#pragma unroll
+  for (int q = 0; q < kS / 4; q++) {
+    const float4 x = __ldg(s4 + q), y = __ldg(t4 + q);
+    sg[4 * q] = x.x, sg[4 * q + 1] = x.y, sg[4 * q + 2] = x.z, sg[4 * q + 3] = x.w;
+    tv[4 * q] = y.x, tv[4 * q + 1] = y.y, tv[4 * q + 2] = y.z, tv[4 * q + 3] = y.w;
+  }
+#pragma unroll
+  for (int q = 0; q < 3 * kS / 4; q++) {
+    const float4 x = __ldg(c4 + q);
+    cl[4 * q] = x.x, cl[4 * q + 1] = x.y, cl[4 * q + 2] = x.z, cl[4 * q + 3] = x.w;
+  }
+  float trans = 1.0f, bg_trans = 1.0f;
+  float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
+#pragma unroll
+  for (int s = 0; s < kS; s++) {
+    bg_trans = trans;
+    const float d = deltas ? tv[s] : clamped_gap(tv, s, kS, vsize);
+    const float opacity = __fsub_rn(1.0f, expf(__fmul_rn(-sg[s], d)));
+    const float w = __fmul_rn(opacity, trans);
+    c0 = __fadd_rn(c0, __fmul_rn(w, cl[3 * s]));
+    c1 = __fadd_rn(c1, __fmul_rn(w, cl[3 * s + 1]));
+    c2 = __fadd_rn(c2, __fmul_rn(w, cl[3 * s + 2]));
+    trans = __fmul_rn(trans, __fadd_rn(__fsub_rn(1.0f, opacity), 1e-10f));
+  }
+  const float bg = white_bg ? 1.0f : 0.0f;
+  color[r * 3 + 0] = __fadd_rn(c0, __fmul_rn(bg_trans, bg));
+  color[r * 3 + 1] = __fadd_rn(c1, __fmul_rn(bg_trans, bg));
+  color[r * 3 + 2] = __fadd_rn(c2, __fmul_rn(bg_trans, bg));
+}
+
 }  // namespace hp
 
 using namespace hp;
@@ -448,7 +494,16 @@ extern "C" int32_t hp_render(const float* deltas, const float* t_val, float vsiz
   if (n_rays == 0) return HP_OK;
   if ((!deltas && !t_val) || !sigmas || !rgbs || !color)
     return set_error(HP_ERR_INVALID_ARGUMENT, "hp_render: null pointer");
-  k_render<<<(unsigned)((n_rays + 255) / 256), 256, 0, (cudaStream_t)stream>>>(deltas, t_val, vsize, sigmas, rgbs,
-                                                                               n_rays, S, white_bg, color);
+  const unsigned blocks = (unsigned)((n_rays + 255) / 256);
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool aligned = (((uintptr_t)(deltas ? deltas : t_val) | (uintptr_t)sigmas | (uintptr_t)rgbs) & 15) == 0;
+  if (aligned && S == 8)
+    k_render_vec<8><<<blocks, 256, 0, st>>>(deltas, t_val, vsize, sigmas, rgbs, n_rays, white_bg, color);
+  else if (aligned && S == 16)
+    k_render_vec<16><<<blocks, 256, 0, st>>>(deltas, t_val, vsize, sigmas, rgbs, n_rays, white_bg, color);
+  else if (aligned && S == 4)
+    k_render_vec<4><<<blocks, 256, 0, st>>>(deltas, t_val, vsize, sigmas, rgbs, n_rays, white_bg, color);
+  else
+    k_render<<<blocks, 256, 0, st>>>(deltas, t_val, vsize, sigmas, rgbs, n_rays, S, white_bg, color);
   return check_launch("k_render");
 }

@@ -65,6 +65,35 @@ def test_feature_query_vs_reference(path):
     _check(out, [g[k] for k in ("pc_xyz", "pc_rgb", "pc_dir", "pc_feat", "out_sp_xyz", "valid", "rays_d")])
 
 
+@pytest.mark.parametrize("S", [4, 8, 16])
+def test_render_vector_loads_match_scalar(S):
+    """The vector-load render (S of 4, 8 or 16 with 16-byte aligned bases) gives the bytes of the
+    scalar render, run on the same values placed 4 bytes past 16-byte alignment: with deltas and
+    with the spacings derived from t_val, black and white background."""
+    g = torch.Generator().manual_seed(S)
+    R = 3001
+    t = torch.sort(torch.rand(R, S, generator=g) * 4, dim=1).values
+    t[::7, -2:] = 0.0  # unfilled samples, as sampling leaves them
+    sig = torch.rand(R, S, generator=g) * 50
+    rgb = torch.rand(R, S, 3, generator=g)
+
+    def off(x):
+        buf = torch.empty(x.numel() + 1, device="cuda")
+        y = buf[1:].view(x.shape)
+        y.copy_(x)
+        return y
+
+    tA, sA, cA = t.cuda(), sig.cuda(), rgb.cuda()
+    d = ops.clamp_t(tA, 0.01)
+    for wb in (False, True):
+        a = ops.render(d, sA, cA, wb)
+        b = ops.render(off(d), off(sA), off(cA), wb)
+        assert np.array_equal(bits(H(a)), bits(H(b)))
+        a = ops.render(None, sA, cA, wb, t_val=tA, vsize=0.01)
+        b = ops.render(None, off(sA), off(cA), wb, t_val=off(tA), vsize=0.01)
+        assert np.array_equal(bits(H(a)), bits(H(b)))
+
+
 @pytest.mark.parametrize("path", downstream_files("render"))
 def test_clamp_t_and_render_vs_reference(path):
     g = np.load(path)
