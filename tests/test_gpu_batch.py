@@ -168,3 +168,38 @@ def test_view_ring_matches_one_stream():
         for a, b in zip(a_view, b_view):
             assert torch.equal(a.view(torch.uint8), b.view(torch.uint8))
     assert any(bool(v[3].any()) for v in got)
+
+
+def test_epcq_calls_over_streams_match_one_stream():
+    """The drop-in epcq calls launch on torch's current stream and take their workspaces and
+    outputs from torch's allocator, so a caller may deal views over several streams: every view's
+    hash table and samples equal those of the same calls on one stream."""
+    from epcq import epcq as E
+    sc = synth.make_shapes(n=60000, n_views=7, width=160, height=128, f=220.0, with_feat=False)
+    model = E.NeuralPoints(pc_type="pc", points=torch.from_numpy(sc.xyz).cuda())
+    opt = E.RenderOptions(kernel_size=5, radius_threshold=0.008, num_sample_points_per_ray=8,
+                          num_point_cloud_per_sp=8)
+    cams = [E.CameraSpec(c2w=D(c.c2w), w2c=D(c.w2c), K=D(c.K), fx=c.fx, fy=c.fy, cx=c.cx, cy=c.cy,
+                         width=c.width, height=c.height) for c in sc.cameras]
+
+    def run(cam):
+        idx, dep, hsh = model.pts2plane(cam, opt)
+        return [idx, dep, hsh, *model.render_image_hashtable_topk(cam, opt, idx, dep, hsh)]
+
+    ref = [run(c) for c in cams]
+    torch.cuda.synchronize()
+    main = torch.cuda.current_stream()
+    side = [torch.cuda.Stream() for _ in range(3)]
+    got = [None] * len(cams)
+    for s in side:
+        s.wait_stream(main)
+    for i, c in enumerate(cams):
+        with torch.cuda.stream(side[i % 3]):
+            got[i] = run(c)
+    for s in side:
+        main.wait_stream(s)
+    torch.cuda.synchronize()
+    for a_view, b_view in zip(ref, got):
+        for a, b in zip(a_view, b_view):
+            assert torch.equal(a.view(torch.uint8), b.view(torch.uint8))
+    assert any(bool(v[6].any()) for v in got)
