@@ -175,18 +175,18 @@ __global__ void __launch_bounds__(256) k_feature_query(FeatArgs a) {
     todo &= todo - 1;
     const int64_t i = i0 + l;
     const int64_t m = __shfl_sync(0xffffffffu, my_off, l);
-    const int64_t ray = i / a.S;
+    const unsigned ray = (unsigned)i / (unsigned)a.S;  // sample counts are below 2^31: 32-bit division
     // sample point and ray direction (generate_rays: ((u - cx) / fx, (v - cy) / fy, 1) rotated by c2w)
     if (lane < 3) a.o_sp[m * 3 + lane] = a.sp_xyz[i * 3 + lane];
     if (lane >= 3 && lane < 6) {
       const int c = lane - 3;
       int u, v;
       if (a.ray_uv) {
-        u = a.ray_uv[2 * ray];
-        v = a.ray_uv[2 * ray + 1];
+        u = a.ray_uv[2 * (int64_t)ray];
+        v = a.ray_uv[2 * (int64_t)ray + 1];
       } else {
-        u = (int)(ray % a.width);
-        v = (int)(ray / a.width);
+        v = (int)(ray / (unsigned)a.width);
+        u = (int)(ray - (unsigned)v * (unsigned)a.width);
       }
       const float dx = __fdiv_rn(__fsub_rn((float)u, a.cx), a.fx);
       const float dy = __fdiv_rn(__fsub_rn((float)v, a.cy), a.fy);
@@ -239,22 +239,23 @@ __global__ void __launch_bounds__(256) k_feature_query_vec(FeatArgs a) {
   const int my_off = valid ? a.offsets[my] : 0;
   const int P = a.P, F = a.feat_dim;
   const int cpp = F * kEsz / 16;  // 16-byte chunks per feature row
+  const int cshift = (cpp & (cpp - 1)) == 0 ? __ffs(cpp) - 1 : -1;  // log2(cpp) when a power of two
   const char* feat = reinterpret_cast<const char*>(a.feat);
   auto one = [&](int l) {
     const int64_t i = i0 + l;
     const int64_t m = __shfl_sync(0xffffffffu, my_off, l);
-    const int64_t ray = i / a.S;
+    const unsigned ray = (unsigned)i / (unsigned)a.S;  // sample counts are below 2^31: 32-bit division
     const int* ids = a.pc_idx + i * P;  // the same few words for every lane (L1)
     if (lane < 3) a.o_sp[m * 3 + lane] = a.sp_xyz[i * 3 + lane];
     if (lane >= 3 && lane < 6) {
       const int c = lane - 3;
       int u, v;
       if (a.ray_uv) {
-        u = a.ray_uv[2 * ray];
-        v = a.ray_uv[2 * ray + 1];
+        u = a.ray_uv[2 * (int64_t)ray];
+        v = a.ray_uv[2 * (int64_t)ray + 1];
       } else {
-        u = (int)(ray % a.width);
-        v = (int)(ray / a.width);
+        v = (int)(ray / (unsigned)a.width);
+        u = (int)(ray - (unsigned)v * (unsigned)a.width);
       }
       const float dx = __fdiv_rn(__fsub_rn((float)u, a.cx), a.fx);
       const float dy = __fdiv_rn(__fsub_rn((float)v, a.cy), a.fy);
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(256) k_feature_query_vec(FeatArgs a) {
     }
     float* of = a.o_feat + m * P * F;
     for (int c = lane; c < P * cpp; c += 32) {
-      const int p = c / cpp, q = c - p * cpp;
+      const int p = cshift >= 0 ? c >> cshift : c / cpp, q = c - p * cpp;
       const int id = ids[p];
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
       if ((unsigned)id < (unsigned)a.n_points)
@@ -308,7 +309,7 @@ __device__ __forceinline__ float clamped_gap(const float* t, int s, int S, float
 __global__ void k_clamp_t(const float* __restrict__ t_val, int64_t rays, int S, float vsize, float* __restrict__ out) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= rays * S) return;
-  const int s = (int)(i % S);
+  const int s = i < 0x7fffffff ? (int)((unsigned)i % (unsigned)S) : (int)(i % S);
   out[i] = clamped_gap(t_val + (i - s), s, S, vsize);
 }
 
