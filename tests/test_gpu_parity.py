@@ -472,3 +472,85 @@ def test_full_size_vs_reference_cuda(name):
             assert np.array_equal(bits(a), bits(b)), nm
         else:
             assert np.array_equal(a, b), nm
+
+
+def _pixel_rays64(cam, u, v):
+    """FP64 pixel-centre rays (origin, unit direction) of the sampling path's definition."""
+    c2w = np.asarray(cam.c2w, np.float64)
+    d = np.stack([(u + 0.5 - cam.cx) / cam.fx, (v + 0.5 - cam.cy) / cam.fy, np.ones_like(u, np.float64)], -1)
+    d = d @ c2w[:3, :3].T
+    return c2w[:3, 3], d / np.linalg.norm(d, axis=-1, keepdims=True)
+
+
+def _ray_dist64(xyz, o, d):
+    e = xyz.astype(np.float64) - o
+    return np.linalg.norm(e - (e @ d)[:, None] * d, axis=-1)
+
+
+@pytest.mark.parametrize("name", ["sphere", "shapes", "clusters"])
+def test_quick_query_sets_vs_brute_force(name):
+    """The listed-ray query at full size against a brute-force FP64 search of each ray's window
+    cells: every returned id lies within the radius of its pixel-centre ray (up to 2e-4 of the
+    radius, the FP32 rounding of the ray and the distance), and every window point more than 2e-4
+    of the radius inside it is returned -- unless the ray's row or one of its cells reached its cap
+    (num_point_per_ray, 32 per cell).  Rays whose windows touch the image border (clamped, so
+    repeated, cells) are left out."""
+    xyz, cam, opt = _full(name)
+    W, Hh, k = cam.width, cam.height, opt.kernel_size
+    lo = (k + 1) // 2 - 1
+    X = D(xyz)
+    sidx, _, hsh = ops.pts2plane(X, D(cam.w2c), D(cam.K), Hh, W, False)
+    rng = np.random.default_rng(11)
+    u = rng.integers(lo, W - (k - 1 - lo), 2048)
+    v = rng.integers(lo, Hh - (k - 1 - lo), 2048)
+    rays = (v * W + u).astype(np.int32)
+    out = H(ops.quick_query(X, D(cam.c2w), cam.fx, cam.fy, cam.cx, cam.cy, W, Hh, opt, sidx, hsh, D(rays)))
+    si, hs = H(sidx), H(hsh).reshape(-1, 2)
+    o, d = _pixel_rays64(cam, u.astype(np.float64), v.astype(np.float64))
+    r, cap, tol = float(opt.radius_threshold), int(opt.num_point_per_ray), 2e-4
+    checked = found = 0
+    for i in range(len(rays)):
+        ids, full_cell = [], False
+        for dv in range(-lo, k - lo):
+            for du in range(-lo, k - lo):
+                s, c = hs[(v[i] + dv) * W + u[i] + du]
+                if s < 0 or c <= 0:
+                    continue
+                cell = si[s:s + c]
+                near = _ray_dist64(xyz[cell], o, d[i]) < r * (1 + tol)
+                full_cell |= int(near.sum()) >= 32
+                ids.append(cell)
+        ids = np.concatenate(ids) if ids else np.zeros(0, np.int32)
+        dist = _ray_dist64(xyz[ids], o, d[i]) if len(ids) else np.zeros(0)
+        got = out[i][out[i] >= 0]
+        assert len(np.unique(got)) == len(got), i  # no repeated cell, so no repeated id
+        assert set(got.tolist()) <= set(ids[dist < r * (1 + tol)].tolist()), i
+        if len(got) < cap and not full_cell:
+            sure = set(ids[dist < r * (1 - tol)].tolist())
+            assert sure <= set(got.tolist()), i
+            checked += 1
+            found += len(sure)
+    assert checked > len(rays) // 2 and found > 0
+
+
+@pytest.mark.parametrize("name", ["sphere", "shapes", "clusters"])
+def test_sample_points_within_radius(name):
+    """Per-sample point selection at full size: every id chosen for an emitted sample lies within
+    the radius of that sample point (FP64 distance, up to 2e-4 of the radius), an emitted sample's
+    ids fill its first slots, and samples that were not emitted carry -1 everywhere."""
+    xyz, cam, opt = _full(name)
+    X = D(xyz)
+    sidx, _, hsh = ops.pts2plane(X, D(cam.w2c), D(cam.K), cam.height, cam.width, False)
+    sp_xyz, pc_idx, sp_t, mask = (H(t) for t in ops.quick_sampling(
+        X, D(cam.c2w), cam.fx, cam.fy, cam.cx, cam.cy, cam.width, cam.height, opt, sidx, hsh))
+    P = pc_idx.shape[-1]
+    m = mask.reshape(-1).astype(bool)
+    idx = pc_idx.reshape(-1, P)
+    assert (idx[~m] == -1).all()
+    ids, sp = idx[m], sp_xyz.reshape(-1, 3)[m].astype(np.float64)
+    valid = ids >= 0
+    # -1 only after the last chosen id of a sample
+    assert not (~valid[:, :-1] & valid[:, 1:]).any()
+    rows, cols = np.nonzero(valid)
+    dist = np.linalg.norm(xyz[ids[rows, cols]].astype(np.float64) - sp[rows], axis=-1)
+    assert len(dist) > 0 and (dist < float(opt.radius_threshold) * (1 + 2e-4)).all()
