@@ -151,6 +151,40 @@ def test_feature_query_edge_cases():
     assert all(t.shape[0] == 0 for t in empty)
 
 
+@pytest.mark.parametrize("dtype,F,P", [(np.float16, 32, 8), (np.float16, 8, 12), (np.float16, 64, 1),
+                                       (np.float32, 32, 8), (np.float32, 4, 3)])
+def test_feature_query_vector_kernel_matches_general(dtype, F, P):
+    """The 16-byte-move gather (feature rows a multiple of 16 bytes, 16-byte aligned bases) gives the
+    bytes of the general gather, which runs on the same feature table placed one element past
+    16-byte alignment: pixel-order and listed rays, ids outside the cloud among the chosen ones."""
+    rng = np.random.default_rng(F * 100 + P)
+    n, R, S, width = 700, 257, 5, 16
+    xyz = rng.standard_normal((n, 3)).astype(np.float32)
+    rgb = rng.random((n, 3), dtype=np.float32)
+    dr = rng.standard_normal((n, 3)).astype(np.float32)
+    feat = rng.standard_normal((n, F)).astype(dtype)
+    sp = rng.standard_normal((R, S, 3)).astype(np.float32)
+    ids = rng.integers(-2, n + 2, size=(R, S, P)).astype(np.int32)
+    mask = rng.random((R, S)) < 0.5
+    c2w = rng.standard_normal((3, 4)).astype(np.float32)
+    uv = np.stack([rng.integers(0, 40, R), rng.integers(0, 30, R)], 1).astype(np.int32)
+
+    def off(a):
+        t = torch.from_numpy(a)
+        buf = torch.empty(t.numel() + 1, dtype=t.dtype, device="cuda")
+        y = buf[1:].view(t.shape)
+        y.copy_(t)
+        return y
+
+    for ray_uv in (None, D(uv)):
+        args = (D(sp), D(ids), D(mask), D(c2w), 50.0, 52.0, 20.0, 15.0, width, ray_uv)
+        a = ops.feature_query(D(xyz), D(rgb), D(dr), D(feat), *args)
+        b = ops.feature_query(D(xyz), D(rgb), D(dr), off(feat), *args)
+        assert a[0].shape[0] == int(mask.sum()) > 0
+        for x, y in zip(a, b):
+            assert torch.equal(x.view(torch.uint8), y.view(torch.uint8))
+
+
 def test_epcq_feature_query_and_render_classes():
     from epcq import epcq as E
     path = downstream_files("feature")[0]
