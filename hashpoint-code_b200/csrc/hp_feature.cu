@@ -223,32 +223,44 @@ __global__ void __launch_bounds__(256) k_feature_query(FeatArgs a) {
 }
 
 // The same gather with 16-byte moves, for feature rows whose bytes are a
-// multiple of 16 (F = 32 fp16 or fp32 features, the Aggregator's width): per
-// valid sample every lane moves 16-byte chunks of the feature rows (fp16
-// chunks widened to two float4 stores), so a sample's features take one
-// gather round instead of one per 32-element pass.
+// multiple of 16 (F = 32 fp16 or fp32 features, the Aggregator's width): the
+// two half-warps serve two valid samples at a time, each lane moving 16-byte
+// chunks of the feature rows (fp16 chunks widened to two float4 stores) and
+// loading its two chunks or elements before storing either, so a pair of
+// samples waits on one round of gathers.
 template <int kHalf>
 __global__ void __launch_bounds__(256) k_feature_query_vec(FeatArgs a) {
   constexpr int kEsz = kHalf ? 2 : 4;
-  const int lane = threadIdx.x & 31;
+  const unsigned kAll = 0xffffffffu;
+  const int lane = threadIdx.x & 31, hl = lane & 15, half = lane >> 4;
   const int64_t i0 = ((int64_t)blockIdx.x * 8 + (threadIdx.x >> 5)) * 32;
   if (i0 >= a.n_samples) return;
   const int64_t my = i0 + lane;
   const bool valid = my < a.n_samples && a.mask[my] != 0;
-  unsigned todo = __ballot_sync(0xffffffffu, valid);
+  unsigned todo = __ballot_sync(kAll, valid);
   const int my_off = valid ? a.offsets[my] : 0;
   const int P = a.P, F = a.feat_dim;
   const int cpp = F * kEsz / 16;  // 16-byte chunks per feature row
   const int cshift = (cpp & (cpp - 1)) == 0 ? __ffs(cpp) - 1 : -1;  // log2(cpp) when a power of two
+  const int nch = P * cpp;
   const char* feat = reinterpret_cast<const char*>(a.feat);
-  auto one = [&](int l) {
+  while (todo) {
+    const int l0 = __ffs(todo) - 1;
+    todo &= todo - 1;
+    int l1 = -1;
+    if (todo) {
+      l1 = __ffs(todo) - 1;
+      todo &= todo - 1;
+    }
+    const int l = half ? l1 : l0;
+    const int64_t m = __shfl_sync(kAll, my_off, l < 0 ? 0 : l);
+    if (l < 0) continue;
     const int64_t i = i0 + l;
-    const int64_t m = __shfl_sync(0xffffffffu, my_off, l);
-    const unsigned ray = (unsigned)i / (unsigned)a.S;  // sample counts are below 2^31: 32-bit division
-    const int* ids = a.pc_idx + i * P;  // the same few words for every lane (L1)
-    if (lane < 3) a.o_sp[m * 3 + lane] = a.sp_xyz[i * 3 + lane];
-    if (lane >= 3 && lane < 6) {
-      const int c = lane - 3;
+    const int* ids = a.pc_idx + i * P;  // the same few words for the half-warp (L1)
+    if (hl < 3) a.o_sp[m * 3 + hl] = a.sp_xyz[i * 3 + hl];
+    if (hl >= 3 && hl < 6) {
+      const int c = hl - 3;
+      const unsigned ray = (unsigned)i / (unsigned)a.S;  // sample counts are below 2^31: 32-bit division
       int u, v;
       if (a.ray_uv) {
         u = a.ray_uv[2 * (int64_t)ray];
@@ -262,39 +274,72 @@ __global__ void __launch_bounds__(256) k_feature_query_vec(FeatArgs a) {
       const float* R = a.c2w + 4 * c;
       a.o_rays[m * 3 + c] = __fadd_rn(__fadd_rn(__fmul_rn(dx, R[0]), __fmul_rn(dy, R[1])), R[2]);
     }
-    for (int e = lane; e < 3 * P; e += 32) {
-      const int p = e / 3, c = e - 3 * p;
-      const int id = ids[p];
-      const bool ok = (unsigned)id < (unsigned)a.n_points;
-      if (c == 0) a.o_valid[m * P + p] = ok;
-      const int64_t o = (m * P + p) * 3 + c;
-      a.o_xyz[o] = ok ? a.xyz[(int64_t)id * 3 + c] : 0.0f;
-      a.o_rgb[o] = ok ? a.rgb[(int64_t)id * 3 + c] : 0.0f;
-      a.o_dir[o] = ok ? a.dir[(int64_t)id * 3 + c] : 0.0f;
-    }
-    float* of = a.o_feat + m * P * F;
-    for (int c = lane; c < P * cpp; c += 32) {
-      const int p = cshift >= 0 ? c >> cshift : c / cpp, q = c - p * cpp;
-      const int id = ids[p];
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if ((unsigned)id < (unsigned)a.n_points)
-        v = __ldg(reinterpret_cast<const uint4*>(feat + ((int64_t)id * cpp + q) * 16));
-      if constexpr (kHalf) {
-        const __half2* h = reinterpret_cast<const __half2*>(&v);
-        const float2 f0 = __half22float2(h[0]), f1 = __half22float2(h[1]), f2 = __half22float2(h[2]),
-                     f3 = __half22float2(h[3]);
-        float4* dst = reinterpret_cast<float4*>(of + p * F + q * 8);
-        dst[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
-        dst[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
-      } else {
-        *reinterpret_cast<uint4*>(of + p * F + q * 4) = v;
+    // xyz / rgb / dir rows: element e = (point, component), two per lane per pass
+    for (int e = hl; e < 3 * P; e += 32) {
+      float x[2], g[2], d[2];
+      bool ok[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int ee = e + 16 * h;
+        x[h] = g[h] = d[h] = 0.0f;
+        ok[h] = false;
+        if (ee < 3 * P) {
+          const int p = ee / 3, c = ee - 3 * p;
+          const int id = ids[p];
+          ok[h] = (unsigned)id < (unsigned)a.n_points;
+          if (ok[h]) {
+            x[h] = a.xyz[(int64_t)id * 3 + c];
+            g[h] = a.rgb[(int64_t)id * 3 + c];
+            d[h] = a.dir[(int64_t)id * 3 + c];
+          }
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int ee = e + 16 * h;
+        if (ee < 3 * P) {
+          const int p = ee / 3, c = ee - 3 * p;
+          if (c == 0) a.o_valid[m * P + p] = ok[h];
+          const int64_t o = (m * P + p) * 3 + c;
+          a.o_xyz[o] = x[h];
+          a.o_rgb[o] = g[h];
+          a.o_dir[o] = d[h];
+        }
       }
     }
-  };
-  while (todo) {
-    const int l = __ffs(todo) - 1;
-    todo &= todo - 1;
-    one(l);
+    // feature rows: chunk q of point p, two per lane per pass
+    float* of = a.o_feat + m * P * F;
+    for (int c = hl; c < nch; c += 32) {
+      uint4 v[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int cc = c + 16 * h;
+        v[h] = make_uint4(0u, 0u, 0u, 0u);
+        if (cc < nch) {
+          const int p = cshift >= 0 ? cc >> cshift : cc / cpp, q = cc - p * cpp;
+          const int id = ids[p];
+          if ((unsigned)id < (unsigned)a.n_points)
+            v[h] = __ldg(reinterpret_cast<const uint4*>(feat + ((int64_t)id * cpp + q) * 16));
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int cc = c + 16 * h;
+        if (cc < nch) {
+          const int p = cshift >= 0 ? cc >> cshift : cc / cpp, q = cc - p * cpp;
+          if constexpr (kHalf) {
+            const __half2* hh = reinterpret_cast<const __half2*>(&v[h]);
+            const float2 f0 = __half22float2(hh[0]), f1 = __half22float2(hh[1]), f2 = __half22float2(hh[2]),
+                         f3 = __half22float2(hh[3]);
+            float4* dst = reinterpret_cast<float4*>(of + p * F + q * 8);
+            dst[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
+            dst[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
+          } else {
+            *reinterpret_cast<uint4*>(of + p * F + q * 4) = v[h];
+          }
+        }
+      }
+    }
   }
 }
 
