@@ -683,7 +683,7 @@ __device__ __forceinline__ unsigned lane_span(int lo, int hi) {
 // A ray costs about ceil(candidates / 32) chunks per pass, so heavy rays finish
 // in a fraction of the time one thread would need for them.
 template <class Src>
-__device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& src, int v, int u) {
+__device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& src, int v, int u, unsigned* wbuf) {
   const unsigned kAll = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
@@ -923,13 +923,19 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
   }
   __syncwarp();
 
-  // per-sample point selection, two samples per pass, buffers fed hits in order
+  // per-sample point selection, two samples per pass, buffers fed hits in
+  // order.  The buffers (distance and id of kBallBuf hits per sample) live in
+  // the serving warp's 32 words of shared memory (wbuf), written by lane 0;
+  // their size, minimum-then-maximum tracking and state are warp-uniform
+  // registers.
+  static_assert(2 * kBallPass * kBallBuf <= 32, "ball buffers exceed the warp's words");
+  float* sbd = reinterpret_cast<float*>(wbuf);              // [kBallPass][kBallBuf] distances
+  int* sbi = reinterpret_cast<int*>(wbuf) + kBallPass * kBallBuf;  // [kBallPass][kBallBuf] ids
   const float omax = fmaxf(fabsf(r.o[0]), fmaxf(fabsf(r.o[1]), fabsf(r.o[2])));
   for (int s0 = 0; s0 < emitted; s0 += kBallPass) {
     const int ns = min(kBallPass, emitted - s0);
     float ts[kBallPass], reach[kBallPass], spx[kBallPass], spy[kBallPass], spz[kBallPass], maxd[kBallPass];
-    float bd[kBallPass][kBallBuf];
-    int bi[kBallPass][kBallBuf], bsize[kBallPass], maxi[kBallPass];
+    int bsize[kBallPass], maxi[kBallPass];
     bool settled[kBallPass];
 #pragma unroll
     for (int q = 0; q < kBallPass; q++) {
@@ -949,8 +955,6 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
       maxi[q] = 0;
       maxd[q] = 1e3f;
       settled[q] = false;
-#pragma unroll
-      for (int e = 0; e < kBallBuf; e++) bd[q][e] = 0.0f, bi[q][e] = -1;
     }
     chunks([&](int, bool valid, int idx, int, int) {
       float dq[kBallPass];
@@ -994,28 +998,30 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
           const float dist = __shfl_sync(kAll, dq[q], l);
           const int cid = __shfl_sync(kAll, id, l);
           if (bsize[q] < kBallBuf) {
-#pragma unroll
-            for (int e = 0; e < kBallBuf; e++)
-              if (e == bsize[q]) bd[q][e] = dist, bi[q][e] = cid;
+            if (lane == 0) {
+              sbd[q * kBallBuf + bsize[q]] = dist;
+              sbi[q * kBallBuf + bsize[q]] = cid;
+            }
             if (maxd[q] > dist) {
               maxd[q] = dist;
               maxi[q] = bsize[q];
             }
             bsize[q]++;
           } else if (dist < maxd[q]) {
+            if (lane == 0) {
+              sbd[q * kBallBuf + maxi[q]] = dist;
+              sbi[q * kBallBuf + maxi[q]] = cid;
+            }
+            __syncwarp();
+            // the new maximum; a scan from the replaced slot's value keeps the
+            // replaced slot when it holds the maximum, else the first slot that does
+            const float ve = lane < kBallBuf ? sbd[q * kBallBuf + lane] : -1.0f;
+            float md = ve;
 #pragma unroll
-            for (int e = 0; e < kBallBuf; e++)
-              if (e == maxi[q]) bd[q][e] = dist, bi[q][e] = cid;
-            float md = dist;
-            int mi = maxi[q];
-#pragma unroll
-            for (int e = 0; e < kBallBuf; e++)
-              if (bd[q][e] > md) {
-                md = bd[q][e];
-                mi = e;
-              }
+            for (int o = 16; o > 0; o >>= 1) md = fmaxf(md, __shfl_xor_sync(kAll, md, o));
+            const unsigned at = __ballot_sync(kAll, lane < kBallBuf && ve == md);
+            maxi[q] = md == dist ? maxi[q] : __ffs(at) - 1;
             maxd[q] = md;
-            maxi[q] = mi;
             settled[q] = true;
           }
         }
@@ -1025,10 +1031,8 @@ __device__ __forceinline__ void sample_ray_warp(const SampleArgs& a, const Src& 
     for (int q = 0; q < kBallPass; q++) {
       if (q >= ns) break;
       int* row = o_idx + (size_t)(s0 + q) * P;
-      int val = -1;
-#pragma unroll
-      for (int e = 0; e < kBallBuf; e++)
-        if (e == lane && e < bsize[q]) val = bi[q][e];
+      __syncwarp();
+      const int val = lane < bsize[q] ? sbi[q * kBallBuf + lane] : -1;
       if (lane < min(P, kBallBuf)) row[lane] = val;
       if (P > kBallBuf)
         for (int e = kBallBuf + lane; e < P; e += 32) row[e] = -1;
@@ -1406,9 +1410,10 @@ __device__ __forceinline__ void process_tile(const SampleArgs& a, Stage<Cfg>& st
     if (h >= nheavy) break;
     const int px = st.order[h];
     if (staged)
-      sample_ray_warp(a, SrcStaged<Cfg>{&st, rv0, ru0, nu}, v0 + px / kTileW, u0 + px % kTileW);
+      sample_ray_warp(a, SrcStaged<Cfg>{&st, rv0, ru0, nu}, v0 + px / kTileW, u0 + px % kTileW,
+                      &st.kept[0][warp * 32]);
     else
-      sample_ray_warp(a, SrcGlobal{}, v0 + px / kTileW, u0 + px % kTileW);
+      sample_ray_warp(a, SrcGlobal{}, v0 + px / kTileW, u0 + px % kTileW, &st.kept[0][warp * 32]);
   }
   __syncthreads();  // the stage is reused by the next tile
 }
